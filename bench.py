@@ -1,0 +1,367 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 lifting DWT on the headline workload:
+
+    2D separable DWT, float32, one 4096 x 4096 image (sum of 32 seeded
+    Gaussian blobs + N(0, 0.01) noise), CDF 9/7, levels (6, 6) on axes (0, 1),
+    boundary Zero; one step = Forward followed by ForwardAdjoint.
+
+Metric: GB/s of algorithmic traffic, 2 * numel * sizeof(float) per transform
+call (one compulsory read and one write of the array), so 268.4 MB per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  N > 1 runs under torchrun, one process per GPU,
+each transforming its own image (independent units, no collective on the
+data path: weak scaling); times are CUDA events, max over ranks.
+`--impl reference` times the reference's own CPU implementation (compiled
+from its sources, oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+N_IMG = 4096
+LEVELS = (6, 6)
+AXES = (0, 1)
+WAVELET = 100907  # CDF9_7
+BC = 0            # Zero
+SEED = 1002
+BYTES_PER_TRANSFORM = 2 * N_IMG * N_IMG * 4
+BYTES_PER_STEP = 2 * BYTES_PER_TRANSFORM
+METRIC = "DWT fwd+adjoint GB/s and %HBM roofline on B200; batched and autograd vs plain"
+WORKLOAD = ("2D separable DWT f32 4096x4096 CDF9_7 levels (6,6) axes (0,1) "
+            "BC Zero, Forward + ForwardAdjoint")
+L2_FLUSH_BYTES = 512 << 20
+
+
+def make_image(seed: int = SEED, n: int = N_IMG) -> np.ndarray:
+    """32 Gaussian blobs (centres U[0,n)^2, sigma U[16,256] px, amplitude
+    N(0,1)) plus N(0, 0.01) noise read as variance 0.01 (sigma 0.1)."""
+    rng = np.random.default_rng(seed)
+    yy = np.arange(n, dtype=np.float32)[:, None]
+    xx = np.arange(n, dtype=np.float32)[None, :]
+    img = np.zeros((n, n), np.float32)
+    for _ in range(32):
+        cy, cx = rng.uniform(0, n, 2)
+        sig = rng.uniform(16, 256)
+        amp = rng.standard_normal()
+        gy = np.exp(-((yy - cy) ** 2) / (2 * sig * sig)).astype(np.float32)
+        gx = np.exp(-((xx - cx) ** 2) / (2 * sig * sig)).astype(np.float32)
+        img += np.float32(amp) * gy * gx
+    img += rng.normal(0, 0.1, (n, n)).astype(np.float32)
+    return img
+
+
+def peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        v = float(json.loads(p.read_text())["hbm_gbs"])
+        return v, "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum)
+    from the committed ncu summary, keyed by kernel name; {} if absent."""
+    out = {}
+    p = ROOT / "profiles" / "traffic_per_launch.txt"
+    if p.exists():
+        for line in p.read_text().splitlines():
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#"):
+                try:
+                    out[(parts[0], parts[1])] = float(parts[2])
+                except ValueError:
+                    pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"lifted_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in self.path.read_text().strip().splitlines()]
+        except OSError:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_time(img: np.ndarray, budget_s: float, min_steps: int = 1):
+    """Times the reference's CPU implementation (oracle/_ref, all host
+    threads) on fwd+adjoint of the image; returns (seconds per step, steps,
+    cores, variant)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    variant = po.best_ref_variant()
+    if variant is None:
+        return None
+    cores = po.nproc()
+    w = np.empty_like(img)
+    y = np.empty_like(img)
+    po.ref_sep(img, WAVELET, 0, BC, list(AXES), list(LEVELS), out=w, variant=variant,
+               nthreads=cores)  # warm the thread pool
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        po.ref_sep(img, WAVELET, 0, BC, list(AXES), list(LEVELS), out=w,
+                   variant=variant, nthreads=cores)
+        po.ref_sep(w, WAVELET, 2, BC, list(AXES), list(LEVELS), out=y,
+                   variant=variant, nthreads=cores)
+        steps += 1
+        el = time.perf_counter() - t0
+        if steps >= min_steps and el >= budget_s:
+            break
+    return el / steps, steps, cores, variant
+
+
+def run_reference_arm(args, rank: int) -> int:
+    if rank != 0:
+        return 0
+    img = make_image()
+    budget = max(1.0, 0.05 * (args.steps + args.warmup))
+    res = cpu_reference_time(img, budget_s=budget, min_steps=args.steps + args.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference CPU build (oracle/_ref) missing or "
+                                         "not executable on this host"}))
+        return 0
+    sec, steps, cores, variant = res
+    gbs = BYTES_PER_STEP / sec / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": 1,
+        "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded blob image)",
+        "config": {"workload": WORKLOAD, "threads": cores,
+                   "build": f"reference sources + Highway stand-in ({variant})"},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{steps} full fwd+adjoint steps on the 4096x4096 image"},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    sys.path.insert(0, str(ROOT))
+    from lifted_b200 import _lib
+    from lifted_b200 import pylifted as pl
+
+    img = make_image(SEED + rank)
+    x = torch.from_numpy(img).to(dev)
+    w = torch.empty_like(x)
+    y = torch.empty_like(x)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def launch_axis(op, src, dst, axis):
+        # One C ABI call per axis (one kernel launch each); exactly the
+        # separable transform, whose later axes work in place on `out`.
+        pl._lwt(src, WAVELET, BC, op, (axis,), (LEVELS[axis],), 1, out=dst)
+
+    def step(evs=None):
+        seq = [(0, x, w, 0), (0, w, w, 1), (2, w, y, 0), (2, y, y, 1)]
+        for i, (op, s, d, a) in enumerate(seq):
+            if evs is not None:
+                evs[i].record(stream)
+            launch_axis(op, s, d, a)
+        if evs is not None:
+            evs[len(seq)].record(stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        step()
+    barrier()
+
+    K = args.steps
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(K)]
+    launches0 = _lib.launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier()
+        for k in range(K):
+            flush.fill_(float(k))  # L2 flush (512 MiB write) outside the events
+            step(events[k])
+        barrier()
+    launches = _lib.launch_count() - launches0
+    clocks = clk.summary()
+
+    step_ms = [ev[0].elapsed_time(ev[4]) for ev in events]
+    per_launch = np.array([[ev[i].elapsed_time(ev[i + 1]) for i in range(4)] for ev in events])
+    total_ms = float(sum(step_ms))
+    t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / K
+    value = world * BYTES_PER_STEP * K / (total_ms / 1e3) / 1e9
+
+    # Roofline of the dominant kernel: the line kernel (every launch here).
+    peak, peak_kind = peak_hbm()
+    mean_launch_ms = per_launch.mean(axis=0)  # fwd ax0, fwd ax1, adj ax0, adj ax1
+    achieved = BYTES_PER_TRANSFORM / 2 / (mean_launch_ms.mean() / 1e3) / 1e9
+    tt = traffic_table()
+    traffic = tt.get(("line_kernel", "cfg2_axis_pass"))
+
+    # End to end through the public API with host (pinned) buffers: each call
+    # copies the image to the GPU, transforms, copies the result back.
+    e2e = None
+    if rank == 0 or world > 1:
+        hx = torch.from_numpy(img).pin_memory().numpy()
+        hw = torch.empty_like(torch.from_numpy(img)).pin_memory().numpy()
+        hy = torch.empty_like(torch.from_numpy(img)).pin_memory().numpy()
+        for _ in range(2):
+            pl.lwt_forward(hx, "cdf9.7", "Zero", axes=AXES, level=LEVELS, out=hw)
+            pl.lwt_forward_adjoint(hw, "cdf9.7", "Zero", axes=AXES, level=LEVELS, out=hy)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            pl.lwt_forward(hx, "cdf9.7", "Zero", axes=AXES, level=LEVELS, out=hw)
+            pl.lwt_forward_adjoint(hw, "cdf9.7", "Zero", axes=AXES, level=LEVELS, out=hy)
+        el = time.perf_counter() - t0
+        te = torch.tensor([el], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        el = float(te.item())
+        e2e = {"value": round(world * BYTES_PER_STEP * args.e2e_steps / el / 1e9, 3),
+               "unit": "GB/s", "h2d_bytes_per_step": 2 * img.nbytes,
+               "d2h_bytes_per_step": 2 * img.nbytes, "steps": args.e2e_steps,
+               "path": "numpy pinned host buffers -> C ABI (staged H2D, kernels, D2H)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        res = cpu_reference_time(img, budget_s=10.0)
+        if res is not None:
+            sec, steps_cpu, cores, variant = res
+            cpu = {"value": round(BYTES_PER_STEP / sec / 1e9, 3), "unit": "GB/s",
+                   "cores": cores, "kind": "reference",
+                   "sample": f"{steps_cpu} full fwd+adjoint steps of the same image "
+                             f"(reference sources + Highway stand-in, {variant}, "
+                             f"{cores} threads)"}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded 32-blob image + noise, seed 1002 + rank)",
+            "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "flushed between steps (512 MiB write outside the timed events)",
+                       "algorithmic_bytes_per_step": BYTES_PER_STEP},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_kind": peak_kind, "kernel": "line_kernel<float>",
+                         "traffic": traffic,
+                         "per_launch_ms": [round(v, 4) for v in mean_launch_ms.tolist()]},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

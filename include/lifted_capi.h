@@ -1,0 +1,165 @@
+/* C ABI of the B200 lifting-scheme DWT library (liblifted_b200.so).
+ *
+ * This is the device boundary of the drop-in: the C++ overloads of
+ * lifted::lwt in lifted.hpp and the Python package lifted_b200 (pylifted
+ * API) both call these functions.  Plain pointers and sizes only; no
+ * exceptions cross this boundary and nothing here aborts.
+ *
+ * Enum values are the reference's (src/lifted-common.hpp:33-98):
+ *   wavelet   lifted::Wavelet            (0 Lazy ... 100907 CDF9_7)
+ *   op        lifted::Transform          0 Forward, 1 Inverse,
+ *                                        2 ForwardAdjoint, 3 InverseAdjoint
+ *   bc        lifted::BoundaryCondition  0 Zero, 1 Constant, 2 Periodic,
+ *                                        3 Symmetric, 4 Reflect
+ * Shapes are in elements; strides are in elements and may be negative.
+ *
+ * Pointers: device (or managed) pointers run asynchronously on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) with no hidden
+ * synchronisation.  Host pointers are staged: the call copies the spanned
+ * input to the GPU, runs, copies the result back and returns after the copy
+ * has finished.  `in == out` with identical strides is allowed (in place).
+ *
+ * Every function returns one of the LIFTED_* status codes below.
+ */
+#ifndef LIFTED_CAPI_H_
+#define LIFTED_CAPI_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define LIFTED_CAPI __declspec(dllexport)
+#else
+#define LIFTED_CAPI __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define LIFTED_OK 0
+/* Invalid argument: unknown wavelet/transform/boundary value, axis >= ndim,
+ * unsupported rank, bad step program. */
+#define LIFTED_EINVAL 1
+/* An input on which the reference hangs, divides by zero or indexes out of
+ * bounds: level 0 with the Lazy wavelet (max_level never returns), a
+ * Periodic/Symmetric/Reflect boundary evaluated on an empty band, Reflect on
+ * a one-element band, the non-separable driver resolving to zero levels.
+ * Nothing is written. */
+#define LIFTED_EDEGENERATE 2
+#define LIFTED_ENOTIMPL 3
+/* A CUDA runtime call failed (the message names it). */
+#define LIFTED_ECUDA 4
+#define LIFTED_ENOMEM 5
+/* A bounded device-side wait gave up. */
+#define LIFTED_ETIMEOUT 6
+/* Request exceeds a stated limit (e.g. the fixed scratch of an entry point
+ * that allocates nothing). */
+#define LIFTED_ETOOLARGE 7
+
+/* A user-defined lifting step (the runtime counterpart of the reference's
+ * compile-time step descriptors, src/lifted-common.hpp:798-1032).
+ *   kind     0 generic update (ntaps coefficients in coef[0..ntaps)),
+ *            1 unit update (y += x[i+offset] or -=, per unit_sub),
+ *            2 repeat update (coef[0] * sum of ntaps neighbours),
+ *            3 scale (ntaps 1: coef[0] = s_mul = d_div; ntaps 2: coef[0] =
+ *              s_mul, coef[1] = d_div)
+ *   target   0 updates the even samples (s), 1 the odd samples (d)
+ *   offset   offset of the first tap relative to the updated index
+ * Coefficients are given as double; casts to float and the 1/c of scale
+ * steps follow the reference (1.0L / c rounded to the element type). */
+typedef struct lifted_step {
+  uint32_t kind;
+  uint32_t target;
+  int32_t offset;
+  uint32_t ntaps;
+  uint32_t unit_sub;
+  uint32_t reserved;
+  double coef[9];
+} lifted_step_t;
+
+#define LIFTED_MAX_TAPS 9
+#define LIFTED_MAX_STEPS 32
+#define LIFTED_MAX_NDIM 16
+
+/* Separable nD transform: every axis in `axes` (in that order) gets the full
+ * levels[i]-level 1D transform; level 0 means max_level(width, length).
+ * Replaces lifted::lwt(..., const size_v& levels, const T* ...) for T = float, double
+ * (src/lifted.hpp:27-39, src/lifted-sep-float.cpp:20-30,
+ * src/lifted-sep-double.cpp:20-30). */
+LIFTED_CAPI int lifted_lwt_sep_f32(uint32_t wavelet, uint32_t op, uint32_t bc,
+                                   size_t ndim, const size_t* shape,
+                                   const ptrdiff_t* stride_in,
+                                   const ptrdiff_t* stride_out, size_t naxes,
+                                   const size_t* axes, const size_t* levels,
+                                   const float* in, float* out, void* stream);
+LIFTED_CAPI int lifted_lwt_sep_f64(uint32_t wavelet, uint32_t op, uint32_t bc,
+                                   size_t ndim, const size_t* shape,
+                                   const ptrdiff_t* stride_in,
+                                   const ptrdiff_t* stride_out, size_t naxes,
+                                   const size_t* axes, const size_t* levels,
+                                   const double* in, double* out,
+                                   void* stream);
+
+/* Non-separable (Mallat) nD transform: `level` levels, each a single-level
+ * transform of every axis over the shrinking approximation corner; level 0
+ * means max_level over the transformed axes.
+ * Replaces lifted::lwt(..., const size_t level, const T* ...) for T = float, double
+ * (src/lifted.hpp:13-25, src/lifted-float.cpp:20-30,
+ * src/lifted-double.cpp:20-30). */
+LIFTED_CAPI int lifted_lwt_f32(uint32_t wavelet, uint32_t op, uint32_t bc,
+                               size_t ndim, const size_t* shape,
+                               const ptrdiff_t* stride_in,
+                               const ptrdiff_t* stride_out, size_t naxes,
+                               const size_t* axes, size_t level,
+                               const float* in, float* out, void* stream);
+LIFTED_CAPI int lifted_lwt_f64(uint32_t wavelet, uint32_t op, uint32_t bc,
+                               size_t ndim, const size_t* shape,
+                               const ptrdiff_t* stride_in,
+                               const ptrdiff_t* stride_out, size_t naxes,
+                               const size_t* axes, size_t level,
+                               const double* in, double* out, void* stream);
+
+/* Separable transform with a caller-supplied step program in place of a
+ * catalogue wavelet (the reference selects its wavelet list at compile time
+ * through the overridable LIFTED_WAVELETS X-macro, src/lifted-common.hpp:33;
+ * a precompiled GPU library takes the program at run time instead).  `width`
+ * is only used when a level is 0.  Steps run in the given order for Forward
+ * and InverseAdjoint and reversed for Inverse and ForwardAdjoint. */
+LIFTED_CAPI int lifted_lwt_sep_program_f32(
+    const lifted_step_t* steps, size_t nsteps, size_t width, uint32_t op,
+    uint32_t bc, size_t ndim, const size_t* shape, const ptrdiff_t* stride_in,
+    const ptrdiff_t* stride_out, size_t naxes, const size_t* axes,
+    const size_t* levels, const float* in, float* out, void* stream);
+LIFTED_CAPI int lifted_lwt_sep_program_f64(
+    const lifted_step_t* steps, size_t nsteps, size_t width, uint32_t op,
+    uint32_t bc, size_t ndim, const size_t* shape, const ptrdiff_t* stride_in,
+    const ptrdiff_t* stride_out, size_t naxes, const size_t* axes,
+    const size_t* levels, const double* in, double* out, void* stream);
+
+/* max_level(width, n) of the reference (src/lifted-common.hpp:1099-1108);
+ * returns (size_t)-1 for width 1, where the reference never returns. */
+LIFTED_CAPI size_t lifted_max_level(size_t width, size_t n);
+/* `width` of a catalogue wavelet (src/lifted-wavelets.hpp), 0 if unknown. */
+LIFTED_CAPI size_t lifted_wavelet_width(uint32_t wavelet);
+/* Number of catalogue wavelets and the enum value of the i-th. */
+LIFTED_CAPI size_t lifted_wavelet_count(void);
+LIFTED_CAPI uint32_t lifted_wavelet_value(size_t index);
+/* Static description of a status code. */
+LIFTED_CAPI const char* lifted_status_string(int status);
+/* Detail of the last failure on the calling thread ("" if none). */
+LIFTED_CAPI const char* lifted_last_error(void);
+/* Number of kernel launches this library has issued from the calling
+ * process (for instrumentation). */
+LIFTED_CAPI uint64_t lifted_launch_count(void);
+/* Process-wide tuning/testing knobs:
+ *   "force_global_scratch" 0/1  keep line buffers in global scratch even
+ *                               when a line fits in shared memory
+ *   "max_global_ctas"      n    CTAs of the global-scratch line path */
+LIFTED_CAPI int lifted_set_option(const char* name, int64_t value);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIFTED_CAPI_H_ */

@@ -1,0 +1,65 @@
+// Host-side interfaces of the B200 lifting DWT library.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/lifted_capi.h"
+#include "lw_types.hpp"
+
+namespace lw {
+
+// One catalogue or user step with its coefficients as long double, exactly
+// as the reference's step factories see them before the cast to T.
+struct StepRow {
+  int kind, target, offset, ntaps, pm;
+  long double c[MAX_TAPS];
+};
+
+struct Program {
+  std::vector<StepRow> rows;
+  size_t width = 0;  // used by max_level (level 0)
+};
+
+// Per-call knobs of the axis passes.
+struct PassOptions {
+  bool force_global = false;   // line buffers in global scratch even if the
+                               // line fits in shared memory (testing)
+  int max_global_ctas = 296;   // CTAs of the global-scratch path
+  void* scratch = nullptr;     // caller-provided scratch (else allocated)
+  size_t scratch_bytes = 0;
+  bool no_alloc = false;       // refuse anything that would allocate
+};
+
+int set_error(int status, const char* fmt, ...);
+void clear_error();
+void count_launches(uint64_t n);
+const char* last_error();
+uint64_t launch_count();
+
+PassOptions default_options();
+int set_option(const char* name, int64_t value);
+
+int catalogue_program(uint32_t wavelet, Program* prog);
+int user_program(const lifted_step_t* steps, size_t nsteps, size_t width,
+                 Program* prog);
+template <typename T>
+void resolve_program(const Program& prog, int op, int across,
+                     DevProgram<T>* out);
+
+size_t max_level(size_t width, size_t n);
+bool line_degenerate(const Program& prog, int op, int bc, int64_t n,
+                     size_t levels);
+size_t wavelet_count();
+uint32_t wavelet_value(size_t i);
+size_t wavelet_width(uint32_t w);
+
+template <typename T>
+int lwt_entry(const Program& prog, bool separable, uint32_t op, uint32_t bc,
+              size_t ndim, const size_t* shape, const ptrdiff_t* sin,
+              const ptrdiff_t* sout, size_t naxes, const size_t* axes,
+              const size_t* levels, size_t level, const T* in, T* out,
+              void* stream, const PassOptions& opt);
+
+}  // namespace lw
