@@ -162,10 +162,14 @@ def test_global_scratch_path_matches_shared_path():
         for w in (2, 100907, 203):
             for bc in range(5):
                 for tf in range(4):
-                    x = rng.standard_normal((3, 1000))
+                    x = rng.standard_normal((5, 1000))
                     rc, o = po.oracle_sep(x, w, tf, bc, [1, 0], [4, 1])
+                    if rc:
+                        with pytest.raises(_lib.LiftedValueError):
+                            gpu_sep(x, w, tf, bc, [1, 0], [4, 1])
+                        continue
                     g = gpu_sep(x, w, tf, bc, [1, 0], [4, 1])
-                    assert rc == 0 and np.array_equal(g, o), (w, bc, tf)
+                    assert np.array_equal(g, o), (w, bc, tf)
     finally:
         _lib.set_option("force_global_scratch", 0)
 
