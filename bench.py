@@ -356,7 +356,7 @@ def main() -> int:
                          "peak_kind": peak_kind, "kernel": "line_kernel<float>",
                          "bytes_per_launch": bytes_per_launch,
                          "traffic": traffic,
-                         "per_launch_ms": [round(v, 4) for v in mean_launch_ms.tolist()]},
+                         "per_axis_pass_ms": [round(v, 4) for v in mean_launch_ms.tolist()]},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),

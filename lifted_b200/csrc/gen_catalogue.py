@@ -97,6 +97,17 @@ def main() -> None:
         c = ", ".join(coefs) if coefs else "0"
         out.append(f"  {{{kind}, {target}, {offset}, {n}, {pm}, {{{c}}}}}, /* {tag} */")
     out.append("#endif")
+    out.append("#ifdef LW_CATALOGUE_SHAPES")
+    out.append("/* structure only (usable in constexpr device code): kind, target, "
+               "offset, ntaps, unit_pm */")
+    for kind, target, offset, n, pm, coefs, tag in rows:
+        out.append(f"  {{{kind}, {target}, {offset}, {n}, {pm}}}, /* {tag} */")
+    out.append("#endif")
+    out.append("#ifdef LW_CATALOGUE_RANGES")
+    out.append("/* first step row, step count, width -- in catalogue order */")
+    for name, value, width, first, count in wavelets:
+        out.append(f"  {{{first}, {count}, {width}}}, /* {name} = {value} */")
+    out.append("#endif")
     out.append("#ifdef LW_CATALOGUE_WAVELETS")
     out.append("/* name, enum value, width, first step row, step count */")
     for name, value, width, first, count in wavelets:

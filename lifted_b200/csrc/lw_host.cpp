@@ -17,6 +17,7 @@
 #include "../../include/lifted_capi.h"
 #include "lw_host.hpp"
 #include "lw_launch.hpp"
+#include "lw_reg.hpp"
 
 static_assert(LDBL_MANT_DIG == 64,
               "the coefficient casts reproduce x86-64 80-bit long double "
@@ -67,6 +68,7 @@ thread_local std::string g_last_error;
 std::atomic<uint64_t> g_launches{0};
 std::atomic<int64_t> g_opt_force_global{0};
 std::atomic<int64_t> g_opt_max_global_ctas{296};
+std::atomic<int64_t> g_opt_fast_path{1};
 
 }  // namespace
 
@@ -88,6 +90,7 @@ int catalogue_program(uint32_t wavelet, Program* prog) {
   if (!w) return set_error(LIFTED_EINVAL, "unknown wavelet value %u", wavelet);
   prog->rows.assign(kCatSteps + w->first, kCatSteps + w->first + w->count);
   prog->width = w->width;
+  prog->cat_index = (int)(w - kCatWavelets);
   return LIFTED_OK;
 }
 
@@ -370,6 +373,39 @@ int run_axis_pass(const Program& prog, int op, int bc, int across,
   p.levels = (int32_t)levels;
   p.bc = bc;
   resolve_program<T>(prog, op, across, &p.prog);
+
+  if (opt.fast_path && !opt.force_global && !opt.no_alloc) {
+    // Overlap of source and destination spans (in place, or aliasing).
+    int64_t ilo = 0, ihi = 0, olo = 0, ohi = 0;
+    for (size_t d = 0; d < ndim; ++d) {
+      const int64_t ei = (shape[d] - 1) * sin[d], eo = (shape[d] - 1) * sout[d];
+      (ei < 0 ? ilo : ihi) += ei;
+      (eo < 0 ? olo : ohi) += eo;
+    }
+    const char* ib = (const char*)(in + ilo);
+    const char* ie = (const char*)(in + ihi + 1);
+    const char* ob = (const char*)(out + olo);
+    const char* oe = (const char*)(out + ohi + 1);
+    const bool overlap = ib < oe && ob < ie;
+    RegPassArgs<T> ra;
+    ra.prog = &p.prog;
+    ra.wi = prog.cat_index;
+    ra.op = op;
+    ra.bc = bc;
+    ra.levels = (int)levels;
+    ra.g = g;
+    ra.in = in;
+    ra.out = out;
+    ra.in_place = overlap;
+    RegStats st;
+    const int rc = plan_reg_pass<T>(ra, stream, &st);
+    count_launches((uint64_t)st.launches);
+    if (rc == 1) return LIFTED_OK;
+    if (rc < 0)
+      return set_error(LIFTED_ECUDA, "register-path launch failed (%d): %s", rc,
+                       rc <= -1000 ? cudaGetErrorString((cudaError_t)(-rc - 1000))
+                                   : "planning error");
+  }
 
   const int64_t n = g.n;
   const int64_t pitch = n;
@@ -741,6 +777,7 @@ PassOptions default_options() {
   PassOptions o;
   o.force_global = g_opt_force_global.load() != 0;
   o.max_global_ctas = (int)g_opt_max_global_ctas.load();
+  o.fast_path = g_opt_fast_path.load() != 0;
   return o;
 }
 
@@ -748,6 +785,8 @@ int set_option(const char* name, int64_t value) {
   if (!name) return set_error(LIFTED_EINVAL, "null option name");
   if (!std::strcmp(name, "force_global_scratch")) {
     g_opt_force_global = value ? 1 : 0;
+  } else if (!std::strcmp(name, "fast_path")) {
+    g_opt_fast_path = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");

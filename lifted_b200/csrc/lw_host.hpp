@@ -19,7 +19,8 @@ struct StepRow {
 
 struct Program {
   std::vector<StepRow> rows;
-  size_t width = 0;  // used by max_level (level 0)
+  size_t width = 0;     // used by max_level (level 0)
+  int cat_index = -1;   // catalogue position; -1 for user programs
 };
 
 // Per-call knobs of the axis passes.
@@ -30,6 +31,7 @@ struct PassOptions {
   void* scratch = nullptr;     // caller-provided scratch (else allocated)
   size_t scratch_bytes = 0;
   bool no_alloc = false;       // refuse anything that would allocate
+  bool fast_path = true;       // use the register-blocked kernels when they apply
 };
 
 int set_error(int status, const char* fmt, ...);

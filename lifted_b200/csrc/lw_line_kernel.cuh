@@ -261,6 +261,71 @@ __device__ __forceinline__ void run_program(const DevProgram<T>& prog, int bc,
     run_step(prog.st[k], prog.normal, prog.across, bc, A, pitch, W, ns, nd);
 }
 
+// Forward-stepping levels on W lines held raw (not yet split) at
+// A + j * pitch, length m each: every level splits A[0..m) into
+// [evens | odds] through B (src/lifted-ops-inl.hpp:104-135), runs the steps
+// and recurses on the evens (src/lifted-drivers-inl.hpp:117-139).  On return
+// A[0..m) holds [a | d_last | ... | d_first] of these levels.
+template <typename T>
+__device__ void coarse_forward(const DevProgram<T>& prog, int bc, T* A,
+                               int64_t pitch, T* B, int64_t pitch_b, int W,
+                               int64_t m, int nlev) {
+  const int tid = threadIdx.x;
+  const int nth = blockDim.x;
+  for (int lvl = 0; lvl < nlev; ++lvl) {
+    const int64_t nd = m / 2, ns = m - nd;
+    const int64_t t2 = (int64_t)W * m;
+    for (int64_t f = tid; f < t2; f += nth) {
+      int j = (int)(f / m);
+      int64_t i = f - (int64_t)j * m;
+      B[j * pitch_b + i] = A[j * pitch + i];
+    }
+    __syncthreads();
+    for (int64_t f = tid; f < t2; f += nth) {
+      int j = (int)(f / m);
+      int64_t i = f - (int64_t)j * m;
+      A[j * pitch + ((i & 1) ? ns + (i >> 1) : (i >> 1))] = B[j * pitch_b + i];
+    }
+    __syncthreads();
+    run_program(prog, bc, A, pitch, W, ns, nd);
+    m = ns;
+  }
+}
+
+// Reverse-stepping levels on W lines: A[0..m0) holds
+// [a | d_last | ... | d_first] of `nlev` levels of a line of length m0; each
+// level runs the (reversed) steps and interleaves s|d through B
+// (src/lifted-drivers-inl.hpp:226-255).  On return A[0..m0) is the line.
+template <typename T>
+__device__ void coarse_reverse(const DevProgram<T>& prog, int bc, T* A,
+                               int64_t pitch, T* B, int64_t pitch_b, int W,
+                               int64_t m0, int nlev) {
+  const int tid = threadIdx.x;
+  const int nth = blockDim.x;
+  int64_t msz[MAX_LEVELS + 1];
+  msz[0] = m0;
+  for (int l = 1; l <= nlev; ++l) msz[l] = msz[l - 1] - msz[l - 1] / 2;
+  for (int lvl = nlev - 1; lvl >= 0; --lvl) {
+    const int64_t m = msz[lvl];
+    const int64_t nd = m / 2, ns = m - nd;
+    run_program(prog, bc, A, pitch, W, ns, nd);
+    const int64_t t2 = (int64_t)W * m;
+    for (int64_t f = tid; f < t2; f += nth) {
+      int j = (int)(f / m);
+      int64_t i = f - (int64_t)j * m;
+      B[j * pitch_b + i] = A[j * pitch + i];
+    }
+    __syncthreads();
+    for (int64_t f = tid; f < t2; f += nth) {
+      int j = (int)(f / m);
+      int64_t i = f - (int64_t)j * m;
+      int64_t src = (i & 1) ? ns + (i >> 1) : (i >> 1);
+      A[j * pitch + i] = B[j * pitch_b + src];
+    }
+    __syncthreads();
+  }
+}
+
 // Base offsets of line `li` in the source and destination.
 __device__ __forceinline__ void line_base(const LineGeom& g, int64_t li,
                                           int64_t& bin, int64_t& bout) {

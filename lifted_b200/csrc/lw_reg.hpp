@@ -1,0 +1,33 @@
+// Host interface of the register-blocked fast path (lw_reg_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lw_types.hpp"
+
+namespace lw {
+
+template <typename T>
+struct RegPassArgs {
+  const DevProgram<T>* prog;  // resolved program for (wavelet, op, T)
+  int wi;                     // catalogue index, -1 for user programs
+  int op;
+  int bc;
+  int levels;                 // levels of this axis pass (>= 1)
+  LineGeom g;
+  const T* in;
+  T* out;
+  bool in_place;              // in and out overlap
+};
+
+struct RegStats {
+  int launches = 0;
+};
+
+// Runs one axis pass on the register path when it applies.  Returns 1 when
+// launched, 0 when the pass is not eligible (the caller falls back to the
+// general line kernel), a negative value on a CUDA failure.
+template <typename T>
+int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats);
+
+}  // namespace lw

@@ -1,0 +1,555 @@
+// Register-blocked lifting kernel of the B200 DWT (the fast path).
+//
+// Each thread owns a contiguous chunk of P (s, d) pairs of one line in
+// registers.  Every lifting step is a register update of the chunk; the few
+// neighbour values a step needs from the adjacent chunks cross through a
+// double-buffered shared-memory mailbox (one block barrier per step).  The
+// split of a level's approximation band into the next level's (s, d) pairs
+// is a register renaming, so consecutive levels run without touching memory;
+// each level's detail band is stored as soon as it is final.  When a level's
+// chunk would fall below the wavelet's reach, the remaining (small) levels
+// finish in shared memory with the exact general step code.
+//
+// The step structure (kind, updated band, offset, tap count, sign) is a
+// compile-time function of the catalogue wavelet and transform; the
+// coefficients come from the host-resolved program.  Arithmetic per element
+// is exactly the reference's Across form (src/lifted-steps-inl.hpp:500-615,
+// 754-885, 1011-1126): sequential fused multiply-adds over the taps, repeat
+// steps summing their taps first.  This kernel serves the Zero boundary,
+// where taps outside the band are skipped and the adjoint folds
+// (src/lifted-steps-inl.hpp:529-546, 576-593) never write, so chunk-local
+// skipping at the band ends reproduces the reference element for element.
+//
+// Modes:
+//   whole line  a CTA holds whole lines (one level-0 line = TPL chunks)
+//   tile        a CTA holds a window [tile start - halo, tile end + halo) of
+//               a long line and runs its first levels; only the tile interior
+//               is stored, the level's approximation band goes to a scratch
+//               band buffer that a whole-line launch finishes.
+// Thread mapping:
+//   contiguous  thread = line * TPL + chunk (lines along a unit-stride axis)
+//   strided     thread = chunk * 32 + line  (32 adjacent lines per CTA: each
+//               load/store instruction covers 32 neighbouring lines)
+#pragma once
+
+#include <cstdint>
+
+#include "lw_line_kernel.cuh"
+#include "lw_types.hpp"
+
+namespace lw {
+
+#ifndef LW_K_GEN
+#define LW_K_GEN 0
+#define LW_K_UNIT 1
+#define LW_K_REPEAT 2
+#define LW_K_SCALE 3
+#define LW_EVENS 0
+#define LW_ODDS 1
+#define LW_PM_ADD 0
+#define LW_PM_SUB 1
+#endif
+
+struct CatShape {
+  int kind, target, offset, ntaps, pm;
+};
+struct CatRange {
+  int first, count, width;
+};
+
+static constexpr CatShape kShapes[] = {
+#define LW_CATALOGUE_SHAPES
+#include "wavelet_catalogue.inc"
+#undef LW_CATALOGUE_SHAPES
+};
+static constexpr CatRange kRanges[] = {
+#define LW_CATALOGUE_RANGES
+#include "wavelet_catalogue.inc"
+#undef LW_CATALOGUE_RANGES
+};
+
+// One step of catalogue wavelet `wi` (catalogue index) for transform `op`,
+// in execution order: the compile-time counterpart of resolve_program().
+struct CStep {
+  int kind, y_is_d, off, ntaps, sub, left, right;
+};
+
+constexpr CStep cstep(int wi, int op, int k) {
+  const bool normal = (op == TF_F || op == TF_I);
+  const bool fwd_tf = (op == TF_F || op == TF_FA);
+  const bool fwd_loop = (op == TF_F || op == TF_IA);
+  const int cnt = kRanges[wi].count;
+  const CatShape s = kShapes[kRanges[wi].first + (fwd_loop ? k : cnt - 1 - k)];
+  CStep c{s.kind, 0, 0, s.kind == K_UNIT ? 1 : s.ntaps, 0, 0, 0};
+  if (s.kind == K_SCALE) return c;
+  const int target = normal ? 1 : 0;
+  c.y_is_d = (s.target == target) ? 1 : 0;
+  c.off = normal ? s.offset : -(c.ntaps - 1 + s.offset);
+  c.sub = (s.kind == K_UNIT) ? (fwd_tf ? s.pm : !s.pm) : (fwd_tf ? 0 : 1);
+  c.left = c.off < 0 ? -c.off : 0;
+  c.right = (c.off + c.ntaps - 1) > 0 ? (c.off + c.ntaps - 1) : 0;
+  return c;
+}
+
+constexpr int cat_nsteps(int wi) { return kRanges[wi].count; }
+
+// Largest distance (in pairs) a step of (wi, op) reaches outside a chunk.
+constexpr int cat_reach(int wi, int op) {
+  int r = 0;
+  for (int k = 0; k < kRanges[wi].count; ++k) {
+    const CStep c = cstep(wi, op, k);
+    if (c.left > r) r = c.left;
+    if (c.right > r) r = c.right;
+  }
+  return r;
+}
+
+// Halo (pairs, per side) that one level of (wi, op) consumes.
+constexpr int cat_level_halo(int wi, int op) {
+  int l = 0, r = 0;
+  for (int k = 0; k < kRanges[wi].count; ++k) {
+    const CStep c = cstep(wi, op, k);
+    l += c.left;
+    r += c.right;
+  }
+  return l > r ? l : r;
+}
+
+template <typename T>
+struct RegParams {
+  const T* in;
+  T* out;
+  T* tmp;                 // tile mode: approximation band of the last level
+  int64_t tmp_line;       // tmp element (line L, position p) at
+  int64_t tmp_pos;        //   tmp[L * tmp_line + p * tmp_pos]
+  LineGeom g;
+  int32_t levels;         // whole line: all levels of the pass
+  int32_t nreg;           // levels run in registers (the finest ones)
+  int32_t tpl;            // chunks per window (threads or warps)
+  int32_t lpc;            // contiguous mode: lines per CTA
+  int64_t tile;           // tile mode: interior length (level-0 elements)
+  int64_t halo;           // tile mode: halo per side, a multiple of 2*P0
+  int64_t ntiles;         // tile mode: tiles per line
+  int32_t vec;            // contiguous unit-stride rows 16-byte aligned
+  int32_t coarse_pitch;   // shared coarse buffer: elements per line (A)
+  int32_t coarse_pitch_b; // and of its split buffer (B)
+  int32_t pad_;
+  DevProgram<T> prog;
+};
+
+namespace reg {
+
+template <typename T>
+struct Ctx {
+  const RegParams<T>* p;
+  T* mb;            // mailbox [2 buffers][2 sides][hmax][nth]
+  T* cA;            // coarse buffers
+  T* cB;
+  int nth, tid, tid_l, tid_r, j, r;
+  bool has_l, has_r, line_ok;
+  int64_t L, bin, bout, n, e0, tile_lo, tile_hi;
+  int buf;
+};
+
+template <typename T>
+__device__ __forceinline__ T tap(const T* xl, const bool* vl, const T* x,
+                                 const T* xr, const bool* vr, int idx, int P,
+                                 int HL, bool& ok) {
+  (void)P;
+  if (idx < 0) {
+    ok = vl[HL + idx];
+    return xl[HL + idx];
+  }
+  if (idx >= P) {
+    ok = vr[idx - P];
+    return xr[idx - P];
+  }
+  ok = true;
+  return x[idx];
+}
+
+// y[0..P) updated from x with one step of compile-time shape CS.
+template <typename T, int P, int PA, int HMAX, int KIND, int OFF, int NT,
+          int SUB, int HL, int HR>
+__device__ __forceinline__ void update(T (&y)[PA], const T (&x)[PA],
+                                       const DevStep<T>& st, Ctx<T>& c,
+                                       int64_t gp0, int64_t nb) {
+  static_assert(HL <= P && HR <= P, "step reaches past the neighbour chunk");
+  const int nth = c.nth;
+  T* mb_first = c.mb + (int64_t)((c.buf * 2 + 0) * HMAX) * nth;
+  T* mb_last = c.mb + (int64_t)((c.buf * 2 + 1) * HMAX) * nth;
+#pragma unroll
+  for (int h = 0; h < HR; ++h) mb_first[h * nth + c.tid] = x[h];
+#pragma unroll
+  for (int h = 0; h < HL; ++h) mb_last[h * nth + c.tid] = x[P - HL + h];
+  __syncthreads();
+  c.buf ^= 1;
+  T xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
+  bool vl[HL > 0 ? HL : 1], vr[HR > 0 ? HR : 1];
+#pragma unroll
+  for (int h = 0; h < HL; ++h) {
+    xl[h] = c.has_l ? mb_last[h * nth + c.tid_l] : T(0);
+    vl[h] = (gp0 - HL + h) >= 0;
+  }
+#pragma unroll
+  for (int h = 0; h < HR; ++h) {
+    xr[h] = c.has_r ? mb_first[h * nth + c.tid_r] : T(0);
+    vr[h] = (gp0 + P + h) < nb;
+  }
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    T yi = y[i];
+    if constexpr (KIND == K_GEN) {
+#pragma unroll
+      for (int k = 0; k < NT; ++k) {
+        bool ok;
+        const T v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok);
+        const T f = fop(SUB, st.c[k], v, yi);
+        yi = ok ? f : yi;
+      }
+    } else if constexpr (KIND == K_REPEAT) {
+      bool ok;
+      T v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok);
+      T x0 = ok ? v : T(0);
+#pragma unroll
+      for (int k = 1; k < NT; ++k) {
+        v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok);
+        x0 = ok ? x0 + v : x0;
+      }
+      yi = fop(SUB, st.c[0], x0, yi);
+    } else {  // unit
+      bool ok;
+      const T v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok);
+      const T f = SUB ? yi - v : yi + v;
+      yi = ok ? f : yi;
+    }
+    y[i] = yi;
+  }
+}
+
+template <typename T, int WI, int OP, int K, int P, int PA, int HMAX>
+__device__ __forceinline__ void steps(T (&s)[PA], T (&d)[PA], Ctx<T>& c,
+                                      int64_t gp0, int64_t nb) {
+  if constexpr (K < cat_nsteps(WI)) {
+    constexpr CStep cs = cstep(WI, OP, K);
+    const DevStep<T>& st = c.p->prog.st[K];
+    if constexpr (cs.kind == K_SCALE) {
+      const T sm = st.sm, dm = st.dm;
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        s[i] = s[i] * sm;
+        d[i] = d[i] * dm;
+      }
+    } else if constexpr (cs.y_is_d) {
+      update<T, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
+             cs.right>(d, s, st, c, gp0, nb);
+    } else {
+      update<T, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
+             cs.right>(s, d, st, c, gp0, nb);
+    }
+    steps<T, WI, OP, K + 1, P, PA, HMAX>(s, d, c, gp0, nb);
+  }
+}
+
+// Stores P consecutive band values v[0..P) at line positions pos0.. of the
+// destination line (vectorised for unit-stride, aligned rows).
+template <typename T, int P, int PA>
+__device__ __forceinline__ void store_run(const T (&v)[PA], Ctx<T>& c,
+                                          int64_t pos0) {
+  const RegParams<T>& p = *c.p;
+  T* o = p.out + c.bout + pos0 * p.g.sout;
+  constexpr int VW = 16 / (int)sizeof(T);
+  if constexpr (P % VW == 0) {
+    if (p.vec && ((pos0 % VW) == 0)) {
+#pragma unroll
+      for (int i = 0; i < P; i += VW) {
+        if constexpr (sizeof(T) == 4) {
+          *reinterpret_cast<float4*>(o + i) =
+              make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        } else {
+          *reinterpret_cast<double2*>(o + i) = make_double2(v[i], v[i + 1]);
+        }
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < P; ++i) o[i * p.g.sout] = v[i];
+}
+
+template <typename T>
+__device__ __forceinline__ bool chunk_stored(const Ctx<T>& c) {
+  return c.line_ok && c.e0 >= c.tile_lo && c.e0 < c.tile_hi;
+}
+
+// Forward-stepping register levels (Forward, InverseAdjoint).
+template <typename T, int WI, int OP, int P0, int HMAX, int LV, bool TILE>
+__device__ __forceinline__ void fwd_levels(T (&s)[P0], T (&d)[P0],
+                                           Ctx<T>& c) {
+  constexpr int P = P0 >> LV;
+  if constexpr (P >= 1 && P >= cat_reach(WI, OP) && LV < MAX_LEVELS) {
+    if (LV < c.p->nreg) {
+      const int64_t nb = c.n >> (LV + 1);
+      const int64_t gp0 = c.e0 >> (LV + 1);
+      steps<T, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
+      if (chunk_stored(c)) store_run<T, P, P0>(d, c, nb + gp0);
+      if (LV + 1 == c.p->nreg) {
+        // hand the approximation band on
+        if (TILE && c.p->nreg < c.p->levels) {
+          if (chunk_stored(c)) {
+            T* t = c.p->tmp + c.L * c.p->tmp_line;
+#pragma unroll
+            for (int i = 0; i < P; ++i) t[(gp0 + i) * c.p->tmp_pos] = s[i];
+          }
+        } else if (TILE) {
+          if (chunk_stored(c)) store_run<T, P, P0>(s, c, gp0);
+        } else if (c.p->nreg == c.p->levels) {
+          if (c.line_ok) store_run<T, P, P0>(s, c, gp0);
+        } else {
+          T* a = c.cA + (int64_t)c.j * c.p->coarse_pitch;
+#pragma unroll
+          for (int i = 0; i < P; ++i) a[gp0 + i] = s[i];
+        }
+        return;
+      }
+#pragma unroll
+      for (int i = 0; i < P / 2; ++i) {
+        d[i] = s[2 * i + 1];
+        s[i] = s[2 * i];
+      }
+      fwd_levels<T, WI, OP, P0, HMAX, LV + 1, TILE>(s, d, c);
+    }
+  }
+}
+
+// Reverse-stepping register levels (Inverse, ForwardAdjoint), coarsest
+// register level first.
+template <typename T, int WI, int OP, int P0, int HMAX, int LV, bool TILE>
+__device__ __forceinline__ void rev_levels(T (&s)[P0], T (&d)[P0],
+                                           Ctx<T>& c) {
+  constexpr int P = P0 >> LV;
+  if constexpr (LV >= 0) {
+    if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+      if (LV < c.p->nreg) {
+        const RegParams<T>& p = *c.p;
+        const int64_t nb = c.n >> (LV + 1);
+        const int64_t gp0 = c.e0 >> (LV + 1);
+        if (LV + 1 == p.nreg) {  // approximation band of the coarsest level
+          if (TILE && p.nreg < p.levels) {
+            const T* t = p.tmp + c.L * p.tmp_line;
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+              const int64_t q = gp0 + i;
+              s[i] = (c.line_ok && q >= 0 && q < nb) ? t[q * p.tmp_pos] : T(0);
+            }
+          } else if (p.nreg == p.levels) {
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+              const int64_t q = gp0 + i;
+              s[i] = (c.line_ok && q >= 0 && q < nb) ? p.in[c.bin + q * p.g.sin]
+                                                     : T(0);
+            }
+          } else {
+            const T* a = c.cA + (int64_t)c.j * p.coarse_pitch;
+#pragma unroll
+            for (int i = 0; i < P; ++i) s[i] = a[gp0 + i];
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+          const int64_t q = gp0 + i;
+          d[i] = (c.line_ok && q >= 0 && q < nb)
+                     ? p.in[c.bin + (nb + q) * p.g.sin]
+                     : T(0);
+        }
+        steps<T, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
+        if constexpr (LV == 0) {
+          if (chunk_stored(c)) {
+            T* o = p.out + c.bout + c.e0 * p.g.sout;
+            constexpr int VW = 16 / (int)sizeof(T);
+            if (p.vec && (c.e0 % VW) == 0) {
+#pragma unroll
+              for (int i = 0; i < P; i += VW / 2) {
+                if constexpr (sizeof(T) == 4) {
+                  *reinterpret_cast<float4*>(o + 2 * i) =
+                      make_float4(s[i], d[i], s[i + 1], d[i + 1]);
+                } else {
+                  *reinterpret_cast<double2*>(o + 2 * i) =
+                      make_double2(s[i], d[i]);
+                }
+              }
+            } else {
+#pragma unroll
+              for (int i = 0; i < P; ++i) {
+                o[(2 * i) * p.g.sout] = s[i];
+                o[(2 * i + 1) * p.g.sout] = d[i];
+              }
+            }
+          }
+        } else {
+#pragma unroll
+          for (int i = P - 1; i >= 0; --i) {
+            s[2 * i + 1] = d[i];
+            s[2 * i] = s[i];
+          }
+        }
+      }
+      if constexpr (LV > 0)
+        rev_levels<T, WI, OP, P0, HMAX, LV - 1, TILE>(s, d, c);
+    } else if constexpr (LV > 0) {
+      rev_levels<T, WI, OP, P0, HMAX, LV - 1, TILE>(s, d, c);
+    }
+  }
+}
+
+}  // namespace reg
+
+// Number of levels the register path can run with P0 pairs per chunk.
+constexpr int reg_max_levels(int wi, int op, int p0) {
+  int lv = 0;
+  const int reach = cat_reach(wi, op);
+  for (int p = p0; p >= 1 && p >= reach && lv < MAX_LEVELS; p >>= 1) ++lv;
+  return lv;
+}
+
+template <typename T, int WI, int OP, int P0, bool STRIDED, bool TILE>
+__global__ void __launch_bounds__(512)
+    reg_kernel(const __grid_constant__ RegParams<T> p) {
+  constexpr int HMAX = cat_reach(WI, OP) > 0 ? cat_reach(WI, OP) : 1;
+  constexpr bool FWD = (OP == TF_F || OP == TF_IA);
+  extern __shared__ __align__(16) unsigned char lw_reg_smem[];
+  reg::Ctx<T> c;
+  c.p = &p;
+  c.nth = blockDim.x;
+  c.tid = threadIdx.x;
+  c.mb = reinterpret_cast<T*>(lw_reg_smem);
+  c.cA = c.mb + 4 * HMAX * c.nth;
+  c.cA = reinterpret_cast<T*>(
+      (reinterpret_cast<uintptr_t>(c.cA) + 15) & ~uintptr_t(15));
+  const int lines_cta = STRIDED ? 32 : p.lpc;
+  c.cB = c.cA + (int64_t)lines_cta * p.coarse_pitch;
+  if (STRIDED) {
+    c.j = c.tid & 31;
+    c.r = c.tid >> 5;
+    c.tid_l = c.tid - 32;
+    c.tid_r = c.tid + 32;
+  } else {
+    c.j = c.tid / p.tpl;
+    c.r = c.tid - c.j * p.tpl;
+    c.tid_l = c.tid - 1;
+    c.tid_r = c.tid + 1;
+  }
+  c.has_l = c.r > 0;
+  c.has_r = c.r < p.tpl - 1;
+  c.buf = 0;
+  int64_t tile_idx = 0, group = blockIdx.x;
+  if (TILE) {
+    tile_idx = blockIdx.x % p.ntiles;
+    group = blockIdx.x / p.ntiles;
+  }
+  c.L = group * lines_cta + c.j;
+  c.line_ok = c.L < p.g.nlines;
+  c.bin = 0;
+  c.bout = 0;
+  if (c.line_ok) line_base(p.g, c.L, c.bin, c.bout);
+  c.n = p.g.n;
+  const int64_t wstart = TILE ? tile_idx * p.tile - p.halo : 0;
+  c.e0 = wstart + (int64_t)2 * P0 * c.r;
+  if (TILE) {
+    c.tile_lo = tile_idx * p.tile;
+    c.tile_hi = c.tile_lo + p.tile < c.n ? c.tile_lo + p.tile : c.n;
+  } else {
+    c.tile_lo = 0;
+    c.tile_hi = c.n;
+  }
+
+  T s[P0], d[P0];
+  if constexpr (FWD) {
+    const bool in_band = c.line_ok && c.e0 >= 0 && c.e0 < c.n;
+    const T* src = p.in + c.bin + c.e0 * p.g.sin;
+    constexpr int VW = 16 / (int)sizeof(T);
+    if (in_band && p.vec && (c.e0 % VW) == 0) {
+#pragma unroll
+      for (int e = 0; e < 2 * P0; e += VW) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 v = *reinterpret_cast<const float4*>(src + e);
+          s[e / 2] = v.x;
+          d[e / 2] = v.y;
+          s[e / 2 + 1] = v.z;
+          d[e / 2 + 1] = v.w;
+        } else {
+          const double2 v = *reinterpret_cast<const double2*>(src + e);
+          s[e / 2] = v.x;
+          d[e / 2] = v.y;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < P0; ++i) {
+        s[i] = in_band ? src[(2 * i) * p.g.sin] : T(0);
+        d[i] = in_band ? src[(2 * i + 1) * p.g.sin] : T(0);
+      }
+    }
+    reg::fwd_levels<T, WI, OP, P0, HMAX, 0, TILE>(s, d, c);
+    if constexpr (!TILE) {
+      if (p.nreg < p.levels) {
+        __syncthreads();
+        const int64_t m = c.n >> p.nreg;
+        coarse_forward(p.prog, BC_ZERO, c.cA, p.coarse_pitch, c.cB,
+                       p.coarse_pitch_b, lines_cta, m, p.levels - p.nreg);
+        // store the coarse region [0, m) of every line of the CTA
+        const int64_t tot = (int64_t)lines_cta * m;
+        for (int64_t f = c.tid; f < tot; f += c.nth) {
+          int jj;
+          int64_t i;
+          if (STRIDED) {
+            i = f / lines_cta;
+            jj = (int)(f - i * lines_cta);
+          } else {
+            jj = (int)(f / m);
+            i = f - (int64_t)jj * m;
+          }
+          const int64_t LL = group * lines_cta + jj;
+          if (LL < p.g.nlines) {
+            int64_t bi, bo;
+            line_base(p.g, LL, bi, bo);
+            p.out[bo + i * p.g.sout] = c.cA[(int64_t)jj * p.coarse_pitch + i];
+          }
+        }
+      }
+    }
+  } else {
+    if constexpr (!TILE) {
+      if (p.nreg < p.levels) {
+        const int64_t m = c.n >> p.nreg;
+        const int64_t tot = (int64_t)lines_cta * m;
+        for (int64_t f = c.tid; f < tot; f += c.nth) {
+          int jj;
+          int64_t i;
+          if (STRIDED) {
+            i = f / lines_cta;
+            jj = (int)(f - i * lines_cta);
+          } else {
+            jj = (int)(f / m);
+            i = f - (int64_t)jj * m;
+          }
+          const int64_t LL = group * lines_cta + jj;
+          T v = T(0);
+          if (LL < p.g.nlines) {
+            int64_t bi, bo;
+            line_base(p.g, LL, bi, bo);
+            v = p.in[bi + i * p.g.sin];
+          }
+          c.cA[(int64_t)jj * p.coarse_pitch + i] = v;
+        }
+        __syncthreads();
+        coarse_reverse(p.prog, BC_ZERO, c.cA, p.coarse_pitch, c.cB,
+                       p.coarse_pitch_b, lines_cta, m, p.levels - p.nreg);
+      }
+    }
+    constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
+    reg::rev_levels<T, WI, OP, P0, HMAX, TOP, TILE>(s, d, c);
+  }
+}
+
+}  // namespace lw

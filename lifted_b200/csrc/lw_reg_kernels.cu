@@ -1,0 +1,331 @@
+// Instantiations and planning of the register-blocked kernel
+// (lw_reg_kernel.cuh).  plan_reg_pass() decides whether one axis pass can run
+// on the register path and launches it; otherwise the caller uses the
+// general line kernel.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+
+#include "lw_launch.hpp"
+#include "lw_reg.hpp"
+#include "lw_reg_kernel.cuh"
+
+namespace lw {
+
+namespace {
+
+// Catalogue indices of the wavelets compiled into the register path.
+constexpr int WI_DB2 = 2;     // Daubechies2
+constexpr int WI_DB4 = 4;     // Daubechies4
+constexpr int WI_CDF97 = 33;  // CDF9_7
+
+template <typename T>
+constexpr int p0_of() {
+  return sizeof(T) == 4 ? 16 : 8;
+}
+
+template <typename T>
+using RegFn = cudaError_t (*)(const RegParams<T>&, int, int, size_t,
+                              cudaStream_t);
+
+template <typename T, int WI, int OP, bool STRIDED, bool TILE>
+cudaError_t launch_one(const RegParams<T>& p, int grid, int block, size_t smem,
+                       cudaStream_t stream) {
+  constexpr int P0 = p0_of<T>();
+  auto kern = reg_kernel<T, WI, OP, P0, STRIDED, TILE>;
+  static bool configured[kMaxDevices] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!configured[dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMaxDynSmem);
+    if (e != cudaSuccess) return e;
+    configured[dev] = true;
+  }
+  kern<<<grid, block, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename T, int WI, int OP>
+RegFn<T> pick_mode(bool strided, bool tile) {
+  if (strided)
+    return tile ? launch_one<T, WI, OP, true, true>
+                : launch_one<T, WI, OP, true, false>;
+  return tile ? launch_one<T, WI, OP, false, true>
+              : launch_one<T, WI, OP, false, false>;
+}
+
+template <typename T, int WI>
+RegFn<T> pick_op(int op, bool strided, bool tile) {
+  switch (op) {
+    case 0: return pick_mode<T, WI, 0>(strided, tile);
+    case 1: return pick_mode<T, WI, 1>(strided, tile);
+    case 2: return pick_mode<T, WI, 2>(strided, tile);
+    default: return pick_mode<T, WI, 3>(strided, tile);
+  }
+}
+
+template <typename T>
+RegFn<T> pick(int wi, int op, bool strided, bool tile) {
+  switch (wi) {
+    case WI_DB2: return pick_op<T, WI_DB2>(op, strided, tile);
+    case WI_DB4: return pick_op<T, WI_DB4>(op, strided, tile);
+    case WI_CDF97: return pick_op<T, WI_CDF97>(op, strided, tile);
+    default: return nullptr;
+  }
+}
+
+bool compiled_wavelet(int wi) {
+  return wi == WI_DB2 || wi == WI_DB4 || wi == WI_CDF97;
+}
+
+// The host-resolved program must have exactly the compile-time structure.
+template <typename T>
+bool structure_matches(const DevProgram<T>& prog, int wi, int op) {
+  if (prog.nsteps != cat_nsteps(wi)) return false;
+  for (int k = 0; k < prog.nsteps; ++k) {
+    const CStep c = cstep(wi, op, k);
+    const DevStep<T>& s = prog.st[k];
+    if (s.kind != c.kind || s.ntaps != c.ntaps) return false;
+    if (c.kind == K_SCALE) continue;
+    if (s.y_is_d != c.y_is_d || s.off != c.off || s.sub != c.sub) return false;
+  }
+  return true;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Unit-stride rows whose line bases are all 16-byte aligned.
+template <typename T>
+bool rows_vectorisable(const LineGeom& g, const T* in, const T* out) {
+  if (g.sin != 1 || g.sout != 1) return false;
+  if (!aligned16(in) || !aligned16(out)) return false;
+  for (int d = 0; d < g.nother; ++d)
+    if (((g.oin[d] * (int64_t)sizeof(T)) & 15) || ((g.oout[d] * (int64_t)sizeof(T)) & 15))
+      return false;
+  return true;
+}
+
+// Lines adjacent in memory along the fastest other dim (both sides).
+bool lines_adjacent(const LineGeom& g) {
+  return g.nother >= 1 && g.oin[0] == 1 && g.oout[0] == 1;
+}
+
+template <typename T>
+size_t reg_smem(int hmax, int block, int lines_cta, int64_t m_coarse,
+                bool coarse) {
+  size_t b = (size_t)4 * hmax * block * sizeof(T) + 16;
+  if (coarse)
+    b += (size_t)lines_cta * (size_t)(m_coarse + (m_coarse + 1) / 2) * sizeof(T);
+  return b;
+}
+
+template <typename T>
+int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
+                 T* out, int levels, bool strided, cudaStream_t stream,
+                 RegStats* stats) {
+  constexpr int P0 = p0_of<T>();
+  const int wi = a.wi, op = a.op;
+  const int64_t n = g.n;
+  if (n % (2 * P0)) return 0;
+  const int64_t tpl = n / (2 * P0);
+  const int maxreg = reg_max_levels(wi, op, P0);
+  const int nreg = levels < maxreg ? levels : maxreg;
+  if (nreg < 1) return 0;
+  int lpc = 1, block;
+  if (strided) {
+    if (tpl > 16) return 0;
+    block = 32 * (int)tpl;
+  } else {
+    if (tpl > 512) return 0;
+    lpc = (int)(256 / tpl);
+    if (lpc < 1) lpc = 1;
+    if (lpc > g.nlines) lpc = (int)g.nlines;
+    block = lpc * (int)tpl;
+  }
+  const int lines_cta = strided ? 32 : lpc;
+  const int64_t m = n >> nreg;
+  const bool coarse = nreg < levels;
+  const int hmax = cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1;
+  const size_t smem = reg_smem<T>(hmax, block, lines_cta, m, coarse);
+  if (smem > kMaxDynSmem) return 0;
+  RegParams<T> p;
+  std::memset(&p, 0, sizeof(p));
+  p.in = in;
+  p.out = out;
+  p.g = g;
+  p.levels = levels;
+  p.nreg = nreg;
+  p.tpl = (int)tpl;
+  p.lpc = lpc;
+  p.vec = (!strided && rows_vectorisable(g, in, out)) ? 1 : 0;
+  p.coarse_pitch = (int)m;
+  p.coarse_pitch_b = (int)((m + 1) / 2);
+  p.prog = *a.prog;
+  const int64_t groups = (g.nlines + lines_cta - 1) / lines_cta;
+  if (groups > 0x7fffffffLL) return 0;
+  RegFn<T> fn = pick<T>(wi, op, strided, false);
+  if (!fn) return 0;
+  cudaError_t e = fn(p, (int)groups, block, smem, stream);
+  if (e != cudaSuccess) return -(int)e - 1000;
+  if (stats) stats->launches += 1;
+  return 1;
+}
+
+// Long lines: tile launch of the first k levels, then a whole-line launch of
+// the rest on the (short) approximation band held in `tmp`.
+template <typename T>
+int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
+                 RegStats* stats) {
+  constexpr int P0 = p0_of<T>();
+  const LineGeom& g = a.g;
+  const int wi = a.wi, op = a.op;
+  const int64_t n = g.n;
+  if (a.in_place) return 0;  // tiles would overwrite other tiles' input
+  if (!lines_adjacent(g)) return 0;
+  if (n % (2 * P0)) return 0;
+  const int maxreg = reg_max_levels(wi, op, P0);
+  // choose k so that the approximation band fits a strided whole-line launch
+  int k = 0;
+  for (int kk = 1; kk <= maxreg && kk <= a.levels; ++kk) {
+    if ((n % ((int64_t)1 << kk)) != 0) break;
+    k = kk;
+    const int64_t m = n >> kk;
+    if (m % (2 * P0) == 0 && m / (2 * P0) <= 16) break;
+  }
+  if (k < 1) return 0;
+  const int64_t m = n >> k;
+  // halo: what k levels consume, rounded up to whole chunks
+  int64_t need = 0;
+  const int lh = cat_level_halo(wi, op);
+  for (int l = 1; l <= k; ++l) need += (int64_t)lh << l;
+  const int64_t chunk = 2 * P0;
+  const int64_t halo = (need + chunk - 1) / chunk * chunk;
+  const int64_t hchunks = halo / chunk;
+  int64_t ichunks = 16 - 2 * hchunks;  // 512 threads at most
+  if (ichunks < 4) return 0;
+  if (ichunks * chunk > n) ichunks = n / chunk;
+  const int64_t tile = ichunks * chunk;
+  const int tpl = (int)(ichunks + 2 * hchunks);
+  const int block = 32 * tpl;
+  const int hmax = cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1;
+  const size_t smem = reg_smem<T>(hmax, block, 32, 0, false);
+  const int64_t ntiles = (n + tile - 1) / tile;
+  const int64_t groups = (g.nlines + 31) / 32;
+  if (groups * ntiles > 0x7fffffffLL) return 0;
+  // the whole-line launch on the approximation band must be possible too
+  if (a.levels > k && ((m % (2 * P0)) || (m / (2 * P0)) > 16)) return 0;
+
+  T* tmp = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (a.levels > k) {
+    const size_t tbytes = (size_t)g.nlines * (size_t)m * sizeof(T);
+    e = cudaMallocAsync((void**)&tmp, tbytes, stream);
+    if (e != cudaSuccess) return -(int)e - 1000;
+  }
+
+  RegParams<T> p;
+  std::memset(&p, 0, sizeof(p));
+  p.g = g;
+  p.tmp = tmp;
+  p.tmp_line = 1;          // tmp is [position][line]: lines adjacent
+  p.tmp_pos = g.nlines;
+  p.nreg = k;
+  p.levels = k;
+  p.tpl = tpl;
+  p.lpc = 32;
+  p.tile = tile;
+  p.halo = halo;
+  p.ntiles = ntiles;
+  p.prog = *a.prog;
+  RegFn<T> tfn = pick<T>(wi, op, true, true);
+  if (!tfn) {
+    if (tmp) cudaFreeAsync(tmp, stream);
+    return 0;
+  }
+  // geometry of the approximation band in tmp: one other dim of nlines
+  // lines (line index L = linear line index of the pass)
+  LineGeom gt;
+  std::memset(&gt, 0, sizeof(gt));
+  gt.n = m;
+  gt.nlines = g.nlines;
+  gt.nother = g.nother;
+  int64_t acc = 1;
+  for (int d = 0; d < g.nother; ++d) {
+    gt.oshape[d] = g.oshape[d];
+    gt.oin[d] = acc;
+    gt.oout[d] = acc;
+    acc *= g.oshape[d];
+  }
+  int rc = 1;
+  const bool fwd = (op == TF_F || op == TF_IA);
+  const bool more = a.levels > k;  // levels left for the whole-line launch
+  p.levels = a.levels;
+  p.in = a.in;
+  p.out = a.out;
+  if (fwd) {
+    e = tfn(p, (int)(groups * ntiles), block, smem, stream);
+    if (e != cudaSuccess) rc = -(int)e - 1000;
+    else if (stats) stats->launches += 1;
+    if (rc == 1 && more) {
+      // levels k+1..: tmp -> the first m positions of every output line
+      LineGeom g2 = gt;
+      g2.sin = g.nlines;
+      g2.sout = g.sout;
+      for (int d = 0; d < g.nother; ++d) g2.oout[d] = g.oout[d];
+      int r2 = launch_whole<T>(a, g2, tmp, a.out, a.levels - k, true, stream, stats);
+      if (r2 != 1) rc = r2 == 0 ? -2 : r2;
+    }
+  } else {
+    if (more) {
+      // coarse levels first: the first m positions of every input line -> tmp
+      LineGeom g2 = gt;
+      g2.sin = g.sin;
+      g2.sout = g.nlines;
+      for (int d = 0; d < g.nother; ++d) g2.oin[d] = g.oin[d];
+      int r2 = launch_whole<T>(a, g2, a.in, tmp, a.levels - k, true, stream, stats);
+      if (r2 != 1) rc = r2 == 0 ? -2 : r2;
+    }
+    if (rc == 1) {
+      e = tfn(p, (int)(groups * ntiles), block, smem, stream);
+      if (e != cudaSuccess) rc = -(int)e - 1000;
+      else if (stats) stats->launches += 1;
+    }
+  }
+  if (tmp) cudaFreeAsync(tmp, stream);
+  return rc;
+}
+
+}  // namespace
+
+template <typename T>
+int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
+                  RegStats* stats) {
+  if (a.bc != BC_ZERO) return 0;
+  if (a.wi < 0 || !compiled_wavelet(a.wi)) return 0;
+  if (a.levels < 1 || a.levels > MAX_LEVELS) return 0;
+  if (!structure_matches(*a.prog, a.wi, a.op)) return 0;
+  const LineGeom& g = a.g;
+  const bool contiguous = (g.sin == 1 && g.sout == 1);
+  // whole lines: contiguous rows, or strided lines adjacent in memory
+  if (contiguous) {
+    int rc = launch_whole<T>(a, g, a.in, a.out, a.levels, false, stream, stats);
+    if (rc != 0) return rc;
+  }
+  if (lines_adjacent(g)) {
+    int rc = launch_whole<T>(a, g, a.in, a.out, a.levels, true, stream, stats);
+    if (rc != 0) return rc;
+    return launch_tiled<T>(a, stream, stats);
+  }
+  return 0;
+}
+
+template int plan_reg_pass<float>(const RegPassArgs<float>&, cudaStream_t,
+                                  RegStats*);
+template int plan_reg_pass<double>(const RegPassArgs<double>&, cudaStream_t,
+                                   RegStats*);
+
+}  // namespace lw

@@ -1,0 +1,98 @@
+"""The register-blocked fast path (whole-line contiguous, whole-line strided
+and tiled strided launches) against the CPU oracle, bit for bit, and against
+the general line kernel (fast path switched off), on shapes that select it:
+lengths that are multiples of the chunk size, Zero boundary, the compiled
+wavelets (Daubechies2, Daubechies4, CDF9_7), all four transforms."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from lifted_b200 import _lib  # noqa: E402
+from lifted_b200 import pylifted as pl  # noqa: E402
+
+WAVELETS = [2, 4, 100907]
+
+
+@pytest.fixture(autouse=True)
+def fast_on():
+    _lib.set_option("fast_path", 1)
+    yield
+    _lib.set_option("fast_path", 1)
+
+
+def run(x, w, tf, bc, axes, levels, fast=True):
+    _lib.set_option("fast_path", 1 if fast else 0)
+    try:
+        t = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+        n0 = _lib.launch_count()
+        y = pl._lwt(t, w, bc, tf, list(axes), list(levels), 1)
+        torch.cuda.synchronize()
+        return y.cpu().numpy(), _lib.launch_count() - n0
+    finally:
+        _lib.set_option("fast_path", 1)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_rows_whole_line(dtype):
+    rng = np.random.default_rng(21)
+    for w in WAVELETS:
+        for n in (32, 64, 256, 1024, 4096):
+            for lv in (1, 2, 3, 5, 6, 9):
+                x = rng.standard_normal((3, n)).astype(dtype)
+                for tf in range(4):
+                    rc, o = po.oracle_sep(x, w, tf, 0, [1], [lv])
+                    if rc:
+                        continue
+                    g, _ = run(x, w, tf, 0, [1], [lv])
+                    assert np.array_equal(g, o), (dtype, w, n, lv, tf)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_columns_whole_and_tiled(dtype):
+    rng = np.random.default_rng(22)
+    for w in WAVELETS:
+        for n in (64, 256, 512, 1024, 2048):
+            for lv in (1, 3, 4, 6):
+                x = rng.standard_normal((n, 40)).astype(dtype)
+                for tf in range(4):
+                    rc, o = po.oracle_sep(x, w, tf, 0, [0], [lv])
+                    if rc:
+                        continue
+                    g, _ = run(x, w, tf, 0, [0], [lv])
+                    assert np.array_equal(g, o), (dtype, w, n, lv, tf)
+
+
+def test_2d_cdf97_like_headline():
+    rng = np.random.default_rng(23)
+    x = rng.standard_normal((1024, 512)).astype(np.float32)
+    for tf in range(4):
+        rc, o = po.oracle_sep(x, 100907, tf, 0, [0, 1], [6, 6])
+        assert rc == 0
+        g, launches = run(x, 100907, tf, 0, [0, 1], [6, 6])
+        assert np.array_equal(g, o), tf
+        g2, _ = run(x, 100907, tf, 0, [0, 1], [6, 6], fast=False)
+        assert np.array_equal(g, g2)
+
+
+def test_3d_db4_fast_path():
+    rng = np.random.default_rng(24)
+    for dtype in (np.float32, np.float64):
+        x = rng.standard_normal((64, 32, 128)).astype(dtype)
+        for tf in (0, 2):
+            rc, o = po.oracle_sep(x, 4, tf, 0, [0, 1, 2], [3, 2, 4])
+            g, _ = run(x, 4, tf, 0, [0, 1, 2], [3, 2, 4])
+            assert rc == 0 and np.array_equal(g, o), (dtype, tf)
+
+
+def test_other_boundaries_fall_back_exactly():
+    rng = np.random.default_rng(25)
+    x = rng.standard_normal((64, 256)).astype(np.float32)
+    for bc in (1, 2, 3, 4):
+        for tf in (0, 2):
+            rc, o = po.oracle_sep(x, 100907, tf, bc, [1, 0], [4, 3])
+            g, _ = run(x, 100907, tf, bc, [1, 0], [4, 3])
+            assert rc == 0 and np.array_equal(g, o), (bc, tf)
