@@ -444,7 +444,7 @@ int run_axis_pass(const Program& prog, int op, int bc, int across,
                          opt.scratch_bytes);
       scratch = (T*)opt.scratch;
     } else {
-      cudaError_t e = cudaMallocAsync((void**)&scratch, bytes, stream);
+      cudaError_t e = scratch_alloc((void**)&scratch, bytes, stream);
       if (e != cudaSuccess)
         return set_error(LIFTED_ENOMEM, "cudaMallocAsync(%zu): %s", bytes,
                          cudaGetErrorString(e));
@@ -457,7 +457,7 @@ int run_axis_pass(const Program& prog, int op, int bc, int across,
   p.nlines_per_cta_stride = (int64_t)grid * W;
   cudaError_t e = launch_line(p, grid, block, smem, stream);
   count_launches(1);
-  if (scratch && !opt.scratch) cudaFreeAsync(scratch, stream);
+  if (scratch && !opt.scratch) scratch_free(scratch, stream);
   if (e != cudaSuccess)
     return set_error(LIFTED_ECUDA, "line kernel launch: %s",
                      cudaGetErrorString(e));
@@ -701,8 +701,8 @@ int lwt_entry(const Program& prog, bool separable, uint32_t op, uint32_t bc,
   T* dbuf_out = nullptr;
   cudaError_t e;
   auto fail = [&](const char* what, cudaError_t err) {
-    if (dbuf_in && !dev_in) cudaFreeAsync(dbuf_in, stream);
-    if (dbuf_out && !dev_out && dbuf_out != dbuf_in) cudaFreeAsync(dbuf_out, stream);
+    if (dbuf_in && !dev_in) scratch_free(dbuf_in, stream);
+    if (dbuf_out && !dev_out && dbuf_out != dbuf_in) scratch_free(dbuf_out, stream);
     cudaStreamSynchronize(stream);
     return set_error(err == cudaErrorMemoryAllocation ? LIFTED_ENOMEM
                                                       : LIFTED_ECUDA,
@@ -711,7 +711,7 @@ int lwt_entry(const Program& prog, bool separable, uint32_t op, uint32_t bc,
   const T* din = in;
   T* dout = out;
   if (!dev_in) {
-    e = cudaMallocAsync((void**)&dbuf_in, ibytes, stream);
+    e = scratch_alloc((void**)&dbuf_in, ibytes, stream);
     if (e != cudaSuccess) return fail("cudaMallocAsync(in)", e);
     e = cudaMemcpyAsync(dbuf_in, in + ilo, ibytes, cudaMemcpyHostToDevice,
                         stream);
@@ -722,7 +722,7 @@ int lwt_entry(const Program& prog, bool separable, uint32_t op, uint32_t bc,
     if (same && !dev_in) {
       dbuf_out = dbuf_in;
     } else {
-      e = cudaMallocAsync((void**)&dbuf_out, obytes, stream);
+      e = scratch_alloc((void**)&dbuf_out, obytes, stream);
       if (e != cudaSuccess) return fail("cudaMallocAsync(out)", e);
       // Prefill when the transform may leave elements of the span untouched:
       // gaps between strided elements, or a first axis with 0 levels (the
@@ -743,8 +743,8 @@ int lwt_entry(const Program& prog, bool separable, uint32_t op, uint32_t bc,
                         stream);
     if (e != cudaSuccess) return fail("cudaMemcpyAsync(D2H out)", e);
   }
-  if (dbuf_in) cudaFreeAsync(dbuf_in, stream);
-  if (dbuf_out && dbuf_out != dbuf_in) cudaFreeAsync(dbuf_out, stream);
+  if (dbuf_in) scratch_free(dbuf_in, stream);
+  if (dbuf_out && dbuf_out != dbuf_in) scratch_free(dbuf_out, stream);
   e = cudaStreamSynchronize(stream);
   if (rc == LIFTED_OK && e != cudaSuccess)
     return set_error(LIFTED_ECUDA, "cudaStreamSynchronize: %s",

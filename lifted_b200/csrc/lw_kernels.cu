@@ -72,4 +72,25 @@ cudaError_t launch_copy(const CopyParams<double>& p, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream) {
+  static bool pool_ready[kMaxDevices] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < kMaxDevices && !pool_ready[dev]) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    pool_ready[dev] = true;
+  }
+  return cudaMallocAsync(p, bytes, stream);
+}
+
+cudaError_t scratch_free(void* p, cudaStream_t stream) {
+  return cudaFreeAsync(p, stream);
+}
+
 }  // namespace lw

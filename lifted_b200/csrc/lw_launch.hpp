@@ -33,6 +33,13 @@ cudaError_t launch_line(const LineParams<float>& p, int grid, int block,
 cudaError_t launch_line(const LineParams<double>& p, int grid, int block,
                         size_t smem, cudaStream_t stream);
 cudaError_t launch_copy(const CopyParams<float>& p, cudaStream_t stream);
+
+// Stream-ordered scratch allocation from the current device's default memory
+// pool.  The first call on a device raises the pool's release threshold so
+// freed scratch stays cached in the pool across synchronisations instead of
+// going back to the driver (a process-local pool attribute).
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream);
+cudaError_t scratch_free(void* p, cudaStream_t stream);
 cudaError_t launch_copy(const CopyParams<double>& p, cudaStream_t stream);
 
 }  // namespace lw

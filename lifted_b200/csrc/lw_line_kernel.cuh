@@ -262,7 +262,7 @@ __device__ __forceinline__ void run_program(const DevProgram<T>& prog, int bc,
 }
 
 // Forward-stepping levels on W lines held raw (not yet split) at
-// A + j * pitch, length m each: every level splits A[0..m) into
+// A + j * pitch, length m each (B needs m elements per line): every level splits A[0..m) into
 // [evens | odds] through B (src/lifted-ops-inl.hpp:104-135), runs the steps
 // and recurses on the evens (src/lifted-drivers-inl.hpp:117-139).  On return
 // A[0..m) holds [a | d_last | ... | d_first] of these levels.
@@ -292,7 +292,8 @@ __device__ void coarse_forward(const DevProgram<T>& prog, int bc, T* A,
   }
 }
 
-// Reverse-stepping levels on W lines: A[0..m0) holds
+// Reverse-stepping levels on W lines (B needs m0 elements per line):
+// A[0..m0) holds
 // [a | d_last | ... | d_first] of `nlev` levels of a line of length m0; each
 // level runs the (reversed) steps and interleaves s|d through B
 // (src/lifted-drivers-inl.hpp:226-255).  On return A[0..m0) is the line.

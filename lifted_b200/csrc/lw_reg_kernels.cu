@@ -10,6 +10,8 @@
 #include "lw_launch.hpp"
 #include "lw_reg.hpp"
 #include "lw_reg_kernel.cuh"
+#include "lw_wrow.hpp"
+#include "lw_wrow_kernel.cuh"
 
 namespace lw {
 
@@ -118,8 +120,8 @@ template <typename T>
 size_t reg_smem(int hmax, int block, int lines_cta, int64_t m_coarse,
                 bool coarse) {
   size_t b = (size_t)4 * hmax * block * sizeof(T) + 16;
-  if (coarse)
-    b += (size_t)lines_cta * (size_t)(m_coarse + (m_coarse + 1) / 2) * sizeof(T);
+  if (coarse)  // A and B, each m elements per line (coarse_forward/_reverse)
+    b += (size_t)lines_cta * (size_t)(2 * m_coarse) * sizeof(T);
   return b;
 }
 
@@ -163,13 +165,47 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   p.lpc = lpc;
   p.vec = (!strided && rows_vectorisable(g, in, out)) ? 1 : 0;
   p.coarse_pitch = (int)m;
-  p.coarse_pitch_b = (int)((m + 1) / 2);
+  p.coarse_pitch_b = (int)m;
   p.prog = *a.prog;
   const int64_t groups = (g.nlines + lines_cta - 1) / lines_cta;
   if (groups > 0x7fffffffLL) return 0;
   RegFn<T> fn = pick<T>(wi, op, strided, false);
   if (!fn) return 0;
   cudaError_t e = fn(p, (int)groups, block, smem, stream);
+  if (e != cudaSuccess) return -(int)e - 1000;
+  if (stats) stats->launches += 1;
+  return 1;
+}
+
+// Contiguous rows of 64 * P0 elements, every level in one warp's registers.
+template <typename T>
+int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
+  const LineGeom& g = a.g;
+  if (!rows_vectorisable(g, a.in, a.out)) return 0;
+  if (g.n % 64) return 0;
+  const int64_t p0 = g.n / 64;
+  const int maxp0 = sizeof(T) == 4 ? 64 : 32;
+  if (p0 < 8 || p0 > maxp0 || (p0 & (p0 - 1))) return 0;
+  const int lv = sizeof(T) == 4 ? wrow_levels_f32(a.wi, a.op, (int)p0)
+                                : wrow_levels_f64(a.wi, a.op, (int)p0);
+  if (lv < a.levels) return 0;
+  WRowParams<T> p;
+  std::memset(&p, 0, sizeof(p));
+  p.in = a.in;
+  p.out = a.out;
+  p.g = g;
+  p.levels = a.levels;
+  p.prog = *a.prog;
+  const int warps = 4;
+  const size_t smem = (size_t)warps * (size_t)g.n * sizeof(T);
+  if (smem > kMaxDynSmem) return 0;
+  const int64_t grid = (g.nlines + warps - 1) / warps;
+  if (grid > 0x7fffffffLL) return 0;
+  cudaError_t e;
+  if constexpr (sizeof(T) == 4)
+    e = launch_wrow_f32(a.wi, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
+  else
+    e = launch_wrow_f64(a.wi, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
   if (stats) stats->launches += 1;
   return 1;
@@ -223,7 +259,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   cudaError_t e = cudaSuccess;
   if (a.levels > k) {
     const size_t tbytes = (size_t)g.nlines * (size_t)m * sizeof(T);
-    e = cudaMallocAsync((void**)&tmp, tbytes, stream);
+    e = scratch_alloc((void**)&tmp, tbytes, stream);
     if (e != cudaSuccess) return -(int)e - 1000;
   }
 
@@ -243,7 +279,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   p.prog = *a.prog;
   RegFn<T> tfn = pick<T>(wi, op, true, true);
   if (!tfn) {
-    if (tmp) cudaFreeAsync(tmp, stream);
+    if (tmp) scratch_free(tmp, stream);
     return 0;
   }
   // geometry of the approximation band in tmp: one other dim of nlines
@@ -295,7 +331,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
       else if (stats) stats->launches += 1;
     }
   }
-  if (tmp) cudaFreeAsync(tmp, stream);
+  if (tmp) scratch_free(tmp, stream);
   return rc;
 }
 
@@ -312,7 +348,9 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
   const bool contiguous = (g.sin == 1 && g.sout == 1);
   // whole lines: contiguous rows, or strided lines adjacent in memory
   if (contiguous) {
-    int rc = launch_whole<T>(a, g, a.in, a.out, a.levels, false, stream, stats);
+    int rc = launch_wrow<T>(a, stream, stats);
+    if (rc != 0) return rc;
+    rc = launch_whole<T>(a, g, a.in, a.out, a.levels, false, stream, stats);
     if (rc != 0) return rc;
   }
   if (lines_adjacent(g)) {

@@ -1,0 +1,78 @@
+// Instantiations of the warp-per-row kernel (lw_wrow_kernel.cuh) for double.
+#include <cuda_runtime.h>
+
+#include "lw_launch.hpp"
+#include "lw_wrow.hpp"
+#include "lw_wrow_kernel.cuh"
+
+namespace lw {
+
+namespace {
+
+template <int WI, int OP, int P0>
+cudaError_t launch_one(const WRowParams<double>& p, int grid, int block,
+                       size_t smem, cudaStream_t stream) {
+  auto kern = wrow_kernel<double, WI, OP, P0>;
+  static bool configured[kMaxDevices] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!configured[dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMaxDynSmem);
+    if (e != cudaSuccess) return e;
+    configured[dev] = true;
+  }
+  kern<<<grid, block, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+using Fn = cudaError_t (*)(const WRowParams<double>&, int, int, size_t, cudaStream_t);
+
+template <int WI, int P0>
+Fn by_op(int op) {
+  switch (op) {
+    case 0: return launch_one<WI, 0, P0>;
+    case 1: return launch_one<WI, 1, P0>;
+    case 2: return launch_one<WI, 2, P0>;
+    default: return launch_one<WI, 3, P0>;
+  }
+}
+
+template <int P0>
+Fn by_wavelet(int wi, int op) {
+  switch (wi) {
+    case 2: return by_op<2, P0>(op);
+    case 4: return by_op<4, P0>(op);
+    case 33: return by_op<33, P0>(op);
+    default: return nullptr;
+  }
+}
+
+}  // namespace
+
+int wrow_levels_f64(int wi, int op, int p0) {
+  switch (p0) {
+    case 8: return (wi == 2 || wi == 4 || wi == 33) ? reg_max_levels(wi, op, 8) : 0;
+    case 16: return (wi == 2 || wi == 4 || wi == 33) ? reg_max_levels(wi, op, 16) : 0;
+    case 32: return (wi == 2 || wi == 4 || wi == 33) ? reg_max_levels(wi, op, 32) : 0;
+    default: return 0;
+  }
+}
+
+cudaError_t launch_wrow_f64(int wi, int op, int p0, const WRowParams<double>& p,
+                            int grid, int block, size_t smem,
+                            cudaStream_t stream) {
+  Fn fn = nullptr;
+  switch (p0) {
+    case 8: fn = by_wavelet<8>(wi, op); break;
+    case 16: fn = by_wavelet<16>(wi, op); break;
+    case 32: fn = by_wavelet<32>(wi, op); break;
+    default: break;
+  }
+  if (!fn) return cudaErrorInvalidValue;
+  return fn(p, grid, block, smem, stream);
+}
+
+}  // namespace lw

@@ -1,0 +1,326 @@
+// Warp-per-row lifting kernel of the B200 DWT (fast path for contiguous rows
+// of 64 * P0 elements).
+//
+// One warp owns one whole row: lane l holds pairs [P0*l, P0*l + P0) of level
+// 1 in registers, and every level of the row runs in those registers.  The
+// neighbour values a lifting step needs cross between lanes by warp shuffles,
+// so the kernel has no block barriers at all; the split of a level's
+// approximation band into the next level's pairs is a register renaming.
+//
+// The row moves through shared memory on both sides: a coalesced cp.async
+// copy (16 bytes per lane, consecutive lanes on consecutive addresses) fills
+// the warp's row buffer, each lane then reads its own contiguous chunk, and
+// the detail bands of every level plus the final approximation are assembled
+// in the same buffer and leave with coalesced 16-byte stores.  The buffer is
+// XOR-swizzled in 16-byte units so that both the coalesced pass and the
+// per-lane chunk pass are free of bank conflicts:
+//   unit U (16 bytes) of the row lives at unit (U & ~7) | ((U ^ swz(U>>3)) & 7)
+//   with swz(R) = (R >> log2(max(1, P0/16))) & 7.
+//
+// Arithmetic per element is the reference's Across form (see
+// lw_reg_kernel.cuh); this kernel serves the Zero boundary, where the lanes
+// at the row ends skip their out-of-band taps.
+#pragma once
+
+#include <cstdint>
+
+#include "lw_reg_kernel.cuh"
+
+namespace lw {
+
+template <typename T>
+struct WRowParams {
+  const T* in;
+  T* out;
+  LineGeom g;        // contiguous rows (g.sin == g.sout == 1)
+  int32_t levels;    // all levels run in registers
+  int32_t pad_;
+  DevProgram<T> prog;
+};
+
+namespace wrow {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// XOR swizzle of 16-byte units for a buffer whose lanes each own a
+// contiguous run of CHUNK elements: unit U of 128-byte row R = U >> 3 lives
+// at (U & ~7) | ((U ^ (R >> SH)) & 7), SH = log2 of the 128-byte rows per
+// lane run (0 when a run is shorter than a row).  Eight consecutive lanes
+// then hit eight distinct 16-byte bank groups both when each lane walks its
+// own run and when consecutive lanes take consecutive units.
+constexpr int swz_shift_bytes(int bytes) {
+  return bytes >= 1024 ? 3 : bytes >= 512 ? 2 : bytes >= 256 ? 1 : 0;
+}
+
+__device__ __forceinline__ int swz(int U, int sh) {
+  const int R = U >> 3;
+  return (U & ~7) | ((U ^ (R >> sh)) & 7);
+}
+
+// Layout of a row read (or written) as runs of CHUNK elements per lane.
+template <typename T, int CHUNK>
+__device__ __forceinline__ T* elem(T* buf, int e) {
+  constexpr int EPU = 16 / (int)sizeof(T);
+  constexpr int SH = swz_shift_bytes(CHUNK * (int)sizeof(T));
+  return buf + swz(e / EPU, SH) * EPU + (e % EPU);
+}
+
+// Banded layout: the approximation [0, nbl) has runs of nbl/32 elements per
+// lane, each detail band [2^k, 2^(k+1)) runs of 2^k/32.  Shift of unit U.
+template <typename T>
+__device__ __forceinline__ int banded_shift(int U, int nbl) {
+  constexpr int EPU = 16 / (int)sizeof(T);
+  const int e = U * EPU;
+  const int region = e < nbl ? nbl : (1 << (31 - __clz(e)));
+  const int bytes = (region / 32) * (int)sizeof(T);
+  return bytes >= 1024 ? 3 : bytes >= 512 ? 2 : bytes >= 256 ? 1 : 0;
+}
+
+// Reads N consecutive elements starting at e (e aligned to min(N, EPU)).
+template <typename T, int CHUNK, int N, int PA>
+__device__ __forceinline__ void read_run(T* buf, int e, T (&v)[PA]) {
+  constexpr int EPU = 16 / (int)sizeof(T);
+  if constexpr (N >= EPU) {
+#pragma unroll
+    for (int i = 0; i < N; i += EPU) {
+      const T* p = elem<T, CHUNK>(buf, e + i);
+      if constexpr (sizeof(T) == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        v[i] = q.x; v[i + 1] = q.y; v[i + 2] = q.z; v[i + 3] = q.w;
+      } else {
+        const double2 q = *reinterpret_cast<const double2*>(p);
+        v[i] = q.x; v[i + 1] = q.y;
+      }
+    }
+  } else if constexpr (N == 2 && sizeof(T) == 4) {
+    const float2 q = *reinterpret_cast<const float2*>(elem<T, CHUNK>(buf, e));
+    v[0] = q.x; v[1] = q.y;
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = *elem<T, CHUNK>(buf, e + i);
+  }
+}
+
+template <typename T, int CHUNK, int N, int PA>
+__device__ __forceinline__ void write_run(T* buf, int e, const T (&v)[PA]) {
+  constexpr int EPU = 16 / (int)sizeof(T);
+  if constexpr (N >= EPU) {
+#pragma unroll
+    for (int i = 0; i < N; i += EPU) {
+      T* p = elem<T, CHUNK>(buf, e + i);
+      if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+      } else {
+        *reinterpret_cast<double2*>(p) = make_double2(v[i], v[i + 1]);
+      }
+    }
+  } else if constexpr (N == 2 && sizeof(T) == 4) {
+    *reinterpret_cast<float2*>(elem<T, CHUNK>(buf, e)) = make_float2(v[0], v[1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) *elem<T, CHUNK>(buf, e + i) = v[i];
+  }
+}
+
+// One step over the lane's P pairs; halos by shuffle.
+template <typename T, int P, int PA, int KIND, int OFF, int NT, int SUB,
+          int HL, int HR>
+__device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
+                                        const DevStep<T>& st, int lane) {
+  static_assert(HL <= P && HR <= P, "step reaches past the neighbour lane");
+  T xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
+#pragma unroll
+  for (int h = 0; h < HL; ++h) xl[h] = __shfl_up_sync(FULL, x[P - HL + h], 1);
+#pragma unroll
+  for (int h = 0; h < HR; ++h) xr[h] = __shfl_down_sync(FULL, x[h], 1);
+  const bool okl = lane > 0, okr = lane < 31;
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    T yi = y[i];
+    if constexpr (KIND == K_GEN) {
+#pragma unroll
+      for (int k = 0; k < NT; ++k) {
+        const int idx = i + OFF + k;
+        const T v = idx < 0 ? xl[HL + idx] : (idx >= P ? xr[idx - P] : x[idx]);
+        const bool ok = idx < 0 ? okl : (idx >= P ? okr : true);
+        const T f = fop(SUB, st.c[k], v, yi);
+        yi = ok ? f : yi;
+      }
+    } else if constexpr (KIND == K_REPEAT) {
+      int idx = i + OFF;
+      T v = idx < 0 ? xl[HL + idx] : (idx >= P ? xr[idx - P] : x[idx]);
+      bool ok = idx < 0 ? okl : (idx >= P ? okr : true);
+      T x0 = ok ? v : T(0);
+#pragma unroll
+      for (int k = 1; k < NT; ++k) {
+        idx = i + OFF + k;
+        v = idx < 0 ? xl[HL + idx] : (idx >= P ? xr[idx - P] : x[idx]);
+        ok = idx < 0 ? okl : (idx >= P ? okr : true);
+        x0 = ok ? x0 + v : x0;
+      }
+      yi = fop(SUB, st.c[0], x0, yi);
+    } else {
+      const int idx = i + OFF;
+      const T v = idx < 0 ? xl[HL + idx] : (idx >= P ? xr[idx - P] : x[idx]);
+      const bool ok = idx < 0 ? okl : (idx >= P ? okr : true);
+      const T f = SUB ? yi - v : yi + v;
+      yi = ok ? f : yi;
+    }
+    y[i] = yi;
+  }
+}
+
+template <typename T, int WI, int OP, int K, int P, int PA>
+__device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
+                                       const DevProgram<T>& prog, int lane) {
+  if constexpr (K < cat_nsteps(WI)) {
+    constexpr CStep cs = cstep(WI, OP, K);
+    const DevStep<T>& st = prog.st[K];
+    if constexpr (cs.kind == K_SCALE) {
+      const T sm = st.sm, dm = st.dm;
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        s[i] = s[i] * sm;
+        d[i] = d[i] * dm;
+      }
+    } else if constexpr (cs.y_is_d) {
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, lane);
+    } else {
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, lane);
+    }
+    wsteps<T, WI, OP, K + 1, P, PA>(s, d, prog, lane);
+  }
+}
+
+// Forward-stepping levels: band of level LV+1 has 32*P pairs.
+template <typename T, int WI, int OP, int P0, int LV>
+__device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
+                                     const DevProgram<T>& prog, int levels,
+                                     int lane) {
+  constexpr int P = P0 >> LV;
+  if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+    if (LV < levels) {
+      constexpr int NB = 32 * P;  // band length at this level
+      wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane);
+      write_run<T, P, P>(buf, NB + P * lane, d);
+      if (LV + 1 == levels) {
+        write_run<T, P, P>(buf, P * lane, s);
+        return;
+      }
+#pragma unroll
+      for (int i = 0; i < P / 2; ++i) {
+        d[i] = s[2 * i + 1];
+        s[i] = s[2 * i];
+      }
+      wfwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane);
+    }
+  }
+}
+
+// Reverse-stepping levels, coarsest first (LV counts down).
+template <typename T, int WI, int OP, int P0, int LV>
+__device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
+                                     const DevProgram<T>& prog, int levels,
+                                     int lane) {
+  constexpr int P = P0 >> LV;
+  if constexpr (LV >= 0) {
+    if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+      if (LV < levels) {
+        constexpr int NB = 32 * P;
+        if (LV + 1 == levels) read_run<T, P, P>(buf, P * lane, s);
+        read_run<T, P, P>(buf, NB + P * lane, d);
+        wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane);
+        if constexpr (LV > 0) {
+#pragma unroll
+          for (int i = P - 1; i >= 0; --i) {
+            s[2 * i + 1] = d[i];
+            s[2 * i] = s[i];
+          }
+        }
+      }
+    }
+    if constexpr (LV > 0) wrev<T, WI, OP, P0, LV - 1>(s, d, buf, prog, levels, lane);
+  }
+}
+
+}  // namespace wrow
+
+// Largest number of levels one warp can run on a row of 64*P0 elements.
+constexpr int wrow_max_levels(int wi, int op, int p0) {
+  return reg_max_levels(wi, op, p0);
+}
+
+template <typename T, int WI, int OP, int P0>
+__global__ void __launch_bounds__(128)
+    wrow_kernel(const __grid_constant__ WRowParams<T> p) {
+  constexpr int N = 64 * P0;                  // row length
+  constexpr int EPU = 16 / (int)sizeof(T);    // elements per 16-byte unit
+  constexpr int UNITS = N / EPU;
+  constexpr bool FWD = (OP == TF_F || OP == TF_IA);
+  extern __shared__ __align__(16) unsigned char lw_wrow_smem[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  if (row >= p.g.nlines) return;  // whole warps only: no block barriers used
+  T* buf = reinterpret_cast<T*>(lw_wrow_smem) + (int64_t)warp * N;
+  int64_t bin, bout;
+  line_base(p.g, row, bin, bout);
+  const T* src = p.in + bin;
+  T* dst = p.out + bout;
+
+  // Approximation band length after the last level (banded layout).
+  const int nbl = N >> p.levels;
+  constexpr int SHA = wrow::swz_shift_bytes(2 * P0 * (int)sizeof(T));
+
+  // coalesced fill: chunk layout (forward reads whole runs of 2*P0) or
+  // banded layout (reverse reads each level's bands)
+#pragma unroll 4
+  for (int u = lane; u < UNITS; u += 32) {
+    const int sh = FWD ? SHA : wrow::banded_shift<T>(u, nbl);
+    const unsigned saddr =
+        (unsigned)__cvta_generic_to_shared(buf + wrow::swz(u, sh) * EPU);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr),
+                 "l"(src + (int64_t)u * EPU)
+                 : "memory");
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncwarp();
+
+  T s[P0], d[P0];
+  if constexpr (FWD) {
+    T x[2 * P0];
+    wrow::read_run<T, 2 * P0, 2 * P0>(buf, 2 * P0 * lane, x);
+#pragma unroll
+    for (int i = 0; i < P0; ++i) {
+      s[i] = x[2 * i];
+      d[i] = x[2 * i + 1];
+    }
+    __syncwarp();
+    wrow::wfwd<T, WI, OP, P0, 0>(s, d, buf, p.prog, p.levels, lane);
+  } else {
+    constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
+    wrow::wrev<T, WI, OP, P0, TOP>(s, d, buf, p.prog, p.levels, lane);
+    __syncwarp();
+    T x[2 * P0];
+#pragma unroll
+    for (int i = 0; i < P0; ++i) {
+      x[2 * i] = s[i];
+      x[2 * i + 1] = d[i];
+    }
+    wrow::write_run<T, 2 * P0, 2 * P0>(buf, 2 * P0 * lane, x);
+  }
+  __syncwarp();
+  // coalesced drain: banded layout (forward) or chunk layout (reverse)
+#pragma unroll 4
+  for (int u = lane; u < UNITS; u += 32) {
+    const int sh = FWD ? wrow::banded_shift<T>(u, nbl) : SHA;
+    const T* q = buf + wrow::swz(u, sh) * EPU;
+    if constexpr (sizeof(T) == 4) {
+      *reinterpret_cast<float4*>(dst + (int64_t)u * EPU) = *reinterpret_cast<const float4*>(q);
+    } else {
+      *reinterpret_cast<double2*>(dst + (int64_t)u * EPU) = *reinterpret_cast<const double2*>(q);
+    }
+  }
+}
+
+}  // namespace lw
