@@ -138,6 +138,31 @@ LIFTED_CAPI int lifted_lwt_sep_program_f64(
     const ptrdiff_t* stride_out, size_t naxes, const size_t* axes,
     const size_t* levels, const double* in, double* out, void* stream);
 
+/* Separable float32 transform that allocates nothing (no counterpart in the
+ * reference, whose CPU transform allocates per-thread line buffers).  For
+ * callers that must not allocate device memory -- a host application that
+ * reserves the GPU's memory for its own allocator and forbids its plugins
+ * from calling cudaMalloc, or a latency-critical loop where an allocation's
+ * implicit synchronisation or failure is unacceptable.  Arguments and
+ * results as lifted_lwt_sep_f32, with these differences:
+ *   - in and out must be device (or managed) pointers; host pointers would
+ *     need staging buffers and are rejected with LIFTED_EINVAL;
+ *   - lines too long for shared memory are buffered in one static device
+ *     array of LIFTED_NOALLOC_SCRATCH_BYTES bytes (held by every GPU that
+ *     loads the library until exit); a line longer than that array can hold
+ *     (LIFTED_NOALLOC_SCRATCH_BYTES / 6 float32 elements, about 5.6 million)
+ *     is rejected with LIFTED_ETOOLARGE;
+ *   - the first call on a device looks up the array's device address, so
+ *     make it before any stream capture;
+ *   - every call shares the array: calls whose kernels overlap on the GPU
+ *     (two streams, two host threads) race and must be serialised. */
+#define LIFTED_NOALLOC_SCRATCH_BYTES (32u << 20)
+LIFTED_CAPI int lifted_lwt_sep_noalloc_f32(
+    uint32_t wavelet, uint32_t op, uint32_t bc, size_t ndim,
+    const size_t* shape, const ptrdiff_t* stride_in,
+    const ptrdiff_t* stride_out, size_t naxes, const size_t* axes,
+    const size_t* levels, const float* in, float* out, void* stream);
+
 /* max_level(width, n) of the reference (src/lifted-common.hpp:1099-1108);
  * returns (size_t)-1 for width 1, where the reference never returns. */
 LIFTED_CAPI size_t lifted_max_level(size_t width, size_t n);

@@ -62,6 +62,7 @@ for _suf in ("f32", "f64"):
     _SIGS[f"lifted_lwt_sep_{_suf}"] = (ctypes.c_int, [_u32, _u32, _u32, _sz, _p, _p, _p, _sz, _p, _p, _p, _p, _p])
     _SIGS[f"lifted_lwt_{_suf}"] = (ctypes.c_int, [_u32, _u32, _u32, _sz, _p, _p, _p, _sz, _p, _sz, _p, _p, _p])
     _SIGS[f"lifted_lwt_sep_program_{_suf}"] = (ctypes.c_int, [_p, _sz, _sz, _u32, _u32, _sz, _p, _p, _p, _sz, _p, _p, _p, _p, _p])
+_SIGS["lifted_lwt_sep_noalloc_f32"] = (ctypes.c_int, [_u32, _u32, _u32, _sz, _p, _p, _p, _sz, _p, _p, _p, _p, _p])
 _SIGS["lifted_max_level"] = (_sz, [_sz, _sz])
 _SIGS["lifted_wavelet_width"] = (_sz, [_u32])
 _SIGS["lifted_wavelet_count"] = (_sz, [])

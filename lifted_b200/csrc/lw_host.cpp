@@ -438,10 +438,14 @@ int run_axis_pass(const Program& prog, int op, int bc, int across,
     grid = (int)std::min<int64_t>(groups, opt.max_global_ctas);
     const size_t bytes = (size_t)grid * line_bytes;
     if (opt.scratch) {
-      if (bytes > opt.scratch_bytes)
+      // Caller-provided scratch of fixed size: as many CTAs as lines fit.
+      const size_t fit = opt.scratch_bytes / line_bytes;
+      if (fit < 1)
         return set_error(LIFTED_ETOOLARGE,
-                         "needs %zu bytes of scratch, %zu available", bytes,
-                         opt.scratch_bytes);
+                         "a line of %lld elements needs %zu bytes of scratch; "
+                         "only %zu are available",
+                         (long long)n, line_bytes, opt.scratch_bytes);
+      if ((size_t)grid > fit) grid = (int)fit;
       scratch = (T*)opt.scratch;
     } else {
       cudaError_t e = scratch_alloc((void**)&scratch, bytes, stream);
