@@ -1,0 +1,62 @@
+// Instantiations of the register-blocked kernel (lw_reg_kernel.cuh) for float.
+#include <cuda_runtime.h>
+
+#include "lw_launch.hpp"
+#include "lw_reg_inst.hpp"
+#include "lw_reg_kernel.cuh"
+
+namespace lw {
+namespace {
+
+constexpr int P0 = 16;
+
+template <int WI, int OP, bool STRIDED, bool TILE, int V>
+cudaError_t launch_one(const RegParams<float>& p, int grid, int block,
+                       size_t smem, cudaStream_t stream) {
+  auto kern = reg_kernel<float, WI, OP, P0, STRIDED, TILE, V>;
+  static bool configured[kMaxDevices] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!configured[dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMaxDynSmem);
+    if (e != cudaSuccess) return e;
+    configured[dev] = true;
+  }
+  kern<<<grid, block, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+template <int WI, int OP>
+RegFn<float> by_mode(bool strided, bool tile, int v) {
+  if (!strided) return tile ? nullptr : launch_one<WI, OP, false, false, 1>;
+  if (v == 2) return tile ? launch_one<WI, OP, true, true, 2>
+                          : launch_one<WI, OP, true, false, 2>;
+  return tile ? launch_one<WI, OP, true, true, 1>
+              : launch_one<WI, OP, true, false, 1>;
+}
+
+template <int WI>
+RegFn<float> by_op(int op, bool strided, bool tile, int v) {
+  switch (op) {
+    case 0: return by_mode<WI, 0>(strided, tile, v);
+    case 1: return by_mode<WI, 1>(strided, tile, v);
+    case 2: return by_mode<WI, 2>(strided, tile, v);
+    default: return by_mode<WI, 3>(strided, tile, v);
+  }
+}
+
+}  // namespace
+
+RegFn<float> pick_reg_f32(int wi, int op, bool strided, bool tile, int v) {
+  switch (wi) {
+    case 2: return by_op<2>(op, strided, tile, v);
+    case 4: return by_op<4>(op, strided, tile, v);
+    case 33: return by_op<33>(op, strided, tile, v);
+    default: return nullptr;
+  }
+}
+
+}  // namespace lw

@@ -137,6 +137,68 @@ struct RegParams {
   DevProgram<T> prog;
 };
 
+// Lane value types: V adjacent lines per lane.  The arithmetic helpers are
+// exact element-wise equivalents of the scalar forms (IEEE round to nearest;
+// packed FP32x2 on sm_100 for float2).
+template <typename T, int V>
+struct LaneVec;
+template <typename T>
+struct LaneVec<T, 1> {
+  using type = T;
+};
+template <>
+struct LaneVec<float, 2> {
+  using type = float2;
+};
+template <>
+struct LaneVec<double, 2> {
+  using type = double2;
+};
+
+__device__ __forceinline__ float vfop(int sub, float c, float x, float y) {
+  return fop(sub, c, x, y);
+}
+__device__ __forceinline__ double vfop(int sub, double c, double x, double y) {
+  return fop(sub, c, x, y);
+}
+__device__ __forceinline__ float2 vfop(int sub, float c, float2 x, float2 y) {
+  const float cc = sub ? -c : c;
+  return __ffma2_rn(make_float2(cc, cc), x, y);
+}
+__device__ __forceinline__ double2 vfop(int sub, double c, double2 x, double2 y) {
+  return make_double2(fop(sub, c, x.x, y.x), fop(sub, c, x.y, y.y));
+}
+__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
+__device__ __forceinline__ double vadd(double a, double b) { return a + b; }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ double2 vadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ float vsub(float a, float b) { return a - b; }
+__device__ __forceinline__ double vsub(double a, double b) { return a - b; }
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) {
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+}
+__device__ __forceinline__ double2 vsub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ double vmul(double a, double b) { return a * b; }
+__device__ __forceinline__ float2 vmul(float2 a, float b) {
+  return __fmul2_rn(a, make_float2(b, b));
+}
+__device__ __forceinline__ double2 vmul(double2 a, double b) {
+  return make_double2(a.x * b, a.y * b);
+}
+template <typename VT>
+__device__ __forceinline__ VT vzero() {
+  return VT{};
+}
+template <typename T>
+__device__ __forceinline__ T vlane(const T& v, int) { return v; }
+__device__ __forceinline__ float vlane(const float2& v, int k) { return k ? v.y : v.x; }
+__device__ __forceinline__ double vlane(const double2& v, int k) { return k ? v.y : v.x; }
+
 namespace reg {
 
 template <typename T>
@@ -151,10 +213,10 @@ struct Ctx {
   int buf;
 };
 
-template <typename T>
-__device__ __forceinline__ T tap(const T* xl, const bool* vl, const T* x,
-                                 const T* xr, const bool* vr, int idx, int P,
-                                 int HL, bool& ok) {
+template <typename VT>
+__device__ __forceinline__ VT tap(const VT* xl, const bool* vl, const VT* x,
+                                  const VT* xr, const bool* vr, int idx, int P,
+                                  int HL, bool& ok) {
   (void)P;
   if (idx < 0) {
     ok = vl[HL + idx];
@@ -169,66 +231,68 @@ __device__ __forceinline__ T tap(const T* xl, const bool* vl, const T* x,
 }
 
 // y[0..P) updated from x with one step of compile-time shape CS.
-template <typename T, int P, int PA, int HMAX, int KIND, int OFF, int NT,
-          int SUB, int HL, int HR>
-__device__ __forceinline__ void update(T (&y)[PA], const T (&x)[PA],
+template <typename T, typename VT, int P, int PA, int HMAX, int KIND, int OFF,
+          int NT, int SUB, int HL, int HR>
+__device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
                                        const DevStep<T>& st, Ctx<T>& c,
                                        int64_t gp0, int64_t nb) {
   static_assert(HL <= P && HR <= P, "step reaches past the neighbour chunk");
   const int nth = c.nth;
-  T* mb_first = c.mb + (int64_t)((c.buf * 2 + 0) * HMAX) * nth;
-  T* mb_last = c.mb + (int64_t)((c.buf * 2 + 1) * HMAX) * nth;
+  VT* mb = reinterpret_cast<VT*>(c.mb);
+  VT* mb_first = mb + (int64_t)((c.buf * 2 + 0) * HMAX) * nth;
+  VT* mb_last = mb + (int64_t)((c.buf * 2 + 1) * HMAX) * nth;
 #pragma unroll
   for (int h = 0; h < HR; ++h) mb_first[h * nth + c.tid] = x[h];
 #pragma unroll
   for (int h = 0; h < HL; ++h) mb_last[h * nth + c.tid] = x[P - HL + h];
   __syncthreads();
   c.buf ^= 1;
-  T xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
+  VT xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
   bool vl[HL > 0 ? HL : 1], vr[HR > 0 ? HR : 1];
 #pragma unroll
   for (int h = 0; h < HL; ++h) {
-    xl[h] = c.has_l ? mb_last[h * nth + c.tid_l] : T(0);
+    xl[h] = c.has_l ? mb_last[h * nth + c.tid_l] : vzero<VT>();
     vl[h] = (gp0 - HL + h) >= 0;
   }
 #pragma unroll
   for (int h = 0; h < HR; ++h) {
-    xr[h] = c.has_r ? mb_first[h * nth + c.tid_r] : T(0);
+    xr[h] = c.has_r ? mb_first[h * nth + c.tid_r] : vzero<VT>();
     vr[h] = (gp0 + P + h) < nb;
   }
 #pragma unroll
   for (int i = 0; i < P; ++i) {
-    T yi = y[i];
+    VT yi = y[i];
     if constexpr (KIND == K_GEN) {
 #pragma unroll
       for (int k = 0; k < NT; ++k) {
         bool ok;
-        const T v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok);
-        const T f = fop(SUB, st.c[k], v, yi);
+        const VT v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok);
+        const VT f = vfop(SUB, st.c[k], v, yi);
         yi = ok ? f : yi;
       }
     } else if constexpr (KIND == K_REPEAT) {
       bool ok;
-      T v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok);
-      T x0 = ok ? v : T(0);
+      VT v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok);
+      VT x0 = ok ? v : vzero<VT>();
 #pragma unroll
       for (int k = 1; k < NT; ++k) {
         v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok);
-        x0 = ok ? x0 + v : x0;
+        x0 = ok ? vadd(x0, v) : x0;
       }
-      yi = fop(SUB, st.c[0], x0, yi);
+      yi = vfop(SUB, st.c[0], x0, yi);
     } else {  // unit
       bool ok;
-      const T v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok);
-      const T f = SUB ? yi - v : yi + v;
+      const VT v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok);
+      const VT f = SUB ? vsub(yi, v) : vadd(yi, v);
       yi = ok ? f : yi;
     }
     y[i] = yi;
   }
 }
 
-template <typename T, int WI, int OP, int K, int P, int PA, int HMAX>
-__device__ __forceinline__ void steps(T (&s)[PA], T (&d)[PA], Ctx<T>& c,
+template <typename T, typename VT, int WI, int OP, int K, int P, int PA,
+          int HMAX>
+__device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
                                       int64_t gp0, int64_t nb) {
   if constexpr (K < cat_nsteps(WI)) {
     constexpr CStep cs = cstep(WI, OP, K);
@@ -237,44 +301,47 @@ __device__ __forceinline__ void steps(T (&s)[PA], T (&d)[PA], Ctx<T>& c,
       const T sm = st.sm, dm = st.dm;
 #pragma unroll
       for (int i = 0; i < P; ++i) {
-        s[i] = s[i] * sm;
-        d[i] = d[i] * dm;
+        s[i] = vmul(s[i], sm);
+        d[i] = vmul(d[i], dm);
       }
     } else if constexpr (cs.y_is_d) {
-      update<T, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
+      update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
              cs.right>(d, s, st, c, gp0, nb);
     } else {
-      update<T, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
+      update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
              cs.right>(s, d, st, c, gp0, nb);
     }
-    steps<T, WI, OP, K + 1, P, PA, HMAX>(s, d, c, gp0, nb);
+    steps<T, VT, WI, OP, K + 1, P, PA, HMAX>(s, d, c, gp0, nb);
   }
 }
 
 // Stores P consecutive band values v[0..P) at line positions pos0.. of the
-// destination line (vectorised for unit-stride, aligned rows).
-template <typename T, int P, int PA>
-__device__ __forceinline__ void store_run(const T (&v)[PA], Ctx<T>& c,
+// destination (vectorised for unit-stride aligned rows; with V lines per
+// lane, one V-wide store per position covers the lane's adjacent lines).
+template <typename T, typename VT, int P, int PA>
+__device__ __forceinline__ void store_run(const VT (&v)[PA], Ctx<T>& c,
                                           int64_t pos0) {
   const RegParams<T>& p = *c.p;
   T* o = p.out + c.bout + pos0 * p.g.sout;
-  constexpr int VW = 16 / (int)sizeof(T);
-  if constexpr (P % VW == 0) {
-    if (p.vec && ((pos0 % VW) == 0)) {
+  if constexpr (sizeof(VT) == sizeof(T)) {
+    constexpr int VW = 16 / (int)sizeof(T);
+    if constexpr (P % VW == 0) {
+      if (p.vec && ((pos0 % VW) == 0)) {
 #pragma unroll
-      for (int i = 0; i < P; i += VW) {
-        if constexpr (sizeof(T) == 4) {
-          *reinterpret_cast<float4*>(o + i) =
-              make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-        } else {
-          *reinterpret_cast<double2*>(o + i) = make_double2(v[i], v[i + 1]);
+        for (int i = 0; i < P; i += VW) {
+          if constexpr (sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(o + i) =
+                make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+          } else {
+            *reinterpret_cast<double2*>(o + i) = make_double2(v[i], v[i + 1]);
+          }
         }
+        return;
       }
-      return;
     }
   }
 #pragma unroll
-  for (int i = 0; i < P; ++i) o[i * p.g.sout] = v[i];
+  for (int i = 0; i < P; ++i) *reinterpret_cast<VT*>(o + i * p.g.sout) = v[i];
 }
 
 template <typename T>
@@ -283,32 +350,37 @@ __device__ __forceinline__ bool chunk_stored(const Ctx<T>& c) {
 }
 
 // Forward-stepping register levels (Forward, InverseAdjoint).
-template <typename T, int WI, int OP, int P0, int HMAX, int LV, bool TILE>
-__device__ __forceinline__ void fwd_levels(T (&s)[P0], T (&d)[P0],
+template <typename T, typename VT, int V, int WI, int OP, int P0, int HMAX,
+          int LV, bool TILE>
+__device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
                                            Ctx<T>& c) {
   constexpr int P = P0 >> LV;
   if constexpr (P >= 1 && P >= cat_reach(WI, OP) && LV < MAX_LEVELS) {
     if (LV < c.p->nreg) {
       const int64_t nb = c.n >> (LV + 1);
       const int64_t gp0 = c.e0 >> (LV + 1);
-      steps<T, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
-      if (chunk_stored(c)) store_run<T, P, P0>(d, c, nb + gp0);
+      steps<T, VT, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
+      if (chunk_stored(c)) store_run<T, VT, P, P0>(d, c, nb + gp0);
       if (LV + 1 == c.p->nreg) {
         // hand the approximation band on
         if (TILE && c.p->nreg < c.p->levels) {
           if (chunk_stored(c)) {
             T* t = c.p->tmp + c.L * c.p->tmp_line;
 #pragma unroll
-            for (int i = 0; i < P; ++i) t[(gp0 + i) * c.p->tmp_pos] = s[i];
+            for (int i = 0; i < P; ++i)
+              *reinterpret_cast<VT*>(t + (gp0 + i) * c.p->tmp_pos) = s[i];
           }
         } else if (TILE) {
-          if (chunk_stored(c)) store_run<T, P, P0>(s, c, gp0);
+          if (chunk_stored(c)) store_run<T, VT, P, P0>(s, c, gp0);
         } else if (c.p->nreg == c.p->levels) {
-          if (c.line_ok) store_run<T, P, P0>(s, c, gp0);
+          if (c.line_ok) store_run<T, VT, P, P0>(s, c, gp0);
         } else {
-          T* a = c.cA + (int64_t)c.j * c.p->coarse_pitch;
 #pragma unroll
-          for (int i = 0; i < P; ++i) a[gp0 + i] = s[i];
+          for (int v = 0; v < V; ++v) {
+            T* a = c.cA + (int64_t)(c.j * V + v) * c.p->coarse_pitch;
+#pragma unroll
+            for (int i = 0; i < P; ++i) a[gp0 + i] = vlane(s[i], v);
+          }
         }
         return;
       }
@@ -317,15 +389,16 @@ __device__ __forceinline__ void fwd_levels(T (&s)[P0], T (&d)[P0],
         d[i] = s[2 * i + 1];
         s[i] = s[2 * i];
       }
-      fwd_levels<T, WI, OP, P0, HMAX, LV + 1, TILE>(s, d, c);
+      fwd_levels<T, VT, V, WI, OP, P0, HMAX, LV + 1, TILE>(s, d, c);
     }
   }
 }
 
 // Reverse-stepping register levels (Inverse, ForwardAdjoint), coarsest
 // register level first.
-template <typename T, int WI, int OP, int P0, int HMAX, int LV, bool TILE>
-__device__ __forceinline__ void rev_levels(T (&s)[P0], T (&d)[P0],
+template <typename T, typename VT, int V, int WI, int OP, int P0, int HMAX,
+          int LV, bool TILE>
+__device__ __forceinline__ void rev_levels(VT (&s)[P0], VT (&d)[P0],
                                            Ctx<T>& c) {
   constexpr int P = P0 >> LV;
   if constexpr (LV >= 0) {
@@ -340,49 +413,59 @@ __device__ __forceinline__ void rev_levels(T (&s)[P0], T (&d)[P0],
 #pragma unroll
             for (int i = 0; i < P; ++i) {
               const int64_t q = gp0 + i;
-              s[i] = (c.line_ok && q >= 0 && q < nb) ? t[q * p.tmp_pos] : T(0);
+              s[i] = (c.line_ok && q >= 0 && q < nb)
+                         ? *reinterpret_cast<const VT*>(t + q * p.tmp_pos)
+                         : vzero<VT>();
             }
           } else if (p.nreg == p.levels) {
 #pragma unroll
             for (int i = 0; i < P; ++i) {
               const int64_t q = gp0 + i;
-              s[i] = (c.line_ok && q >= 0 && q < nb) ? p.in[c.bin + q * p.g.sin]
-                                                     : T(0);
+              s[i] = (c.line_ok && q >= 0 && q < nb)
+                         ? *reinterpret_cast<const VT*>(p.in + c.bin + q * p.g.sin)
+                         : vzero<VT>();
             }
           } else {
-            const T* a = c.cA + (int64_t)c.j * p.coarse_pitch;
 #pragma unroll
-            for (int i = 0; i < P; ++i) s[i] = a[gp0 + i];
+            for (int i = 0; i < P; ++i) {
+              if constexpr (V == 1) {
+                s[i] = c.cA[(int64_t)c.j * p.coarse_pitch + gp0 + i];
+              } else {
+                const T* a0 = c.cA + (int64_t)(c.j * V) * p.coarse_pitch;
+                s[i] = VT{a0[gp0 + i], a0[p.coarse_pitch + gp0 + i]};
+              }
+            }
           }
         }
 #pragma unroll
         for (int i = 0; i < P; ++i) {
           const int64_t q = gp0 + i;
           d[i] = (c.line_ok && q >= 0 && q < nb)
-                     ? p.in[c.bin + (nb + q) * p.g.sin]
-                     : T(0);
+                     ? *reinterpret_cast<const VT*>(p.in + c.bin + (nb + q) * p.g.sin)
+                     : vzero<VT>();
         }
-        steps<T, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
+        steps<T, VT, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
         if constexpr (LV == 0) {
           if (chunk_stored(c)) {
             T* o = p.out + c.bout + c.e0 * p.g.sout;
             constexpr int VW = 16 / (int)sizeof(T);
-            if (p.vec && (c.e0 % VW) == 0) {
+            if (V == 1 && p.vec && (c.e0 % VW) == 0) {
 #pragma unroll
               for (int i = 0; i < P; i += VW / 2) {
                 if constexpr (sizeof(T) == 4) {
                   *reinterpret_cast<float4*>(o + 2 * i) =
-                      make_float4(s[i], d[i], s[i + 1], d[i + 1]);
+                      make_float4(vlane(s[i], 0), vlane(d[i], 0),
+                                  vlane(s[i + 1], 0), vlane(d[i + 1], 0));
                 } else {
                   *reinterpret_cast<double2*>(o + 2 * i) =
-                      make_double2(s[i], d[i]);
+                      make_double2(vlane(s[i], 0), vlane(d[i], 0));
                 }
               }
             } else {
 #pragma unroll
               for (int i = 0; i < P; ++i) {
-                o[(2 * i) * p.g.sout] = s[i];
-                o[(2 * i + 1) * p.g.sout] = d[i];
+                *reinterpret_cast<VT*>(o + (2 * i) * p.g.sout) = s[i];
+                *reinterpret_cast<VT*>(o + (2 * i + 1) * p.g.sout) = d[i];
               }
             }
           }
@@ -395,9 +478,9 @@ __device__ __forceinline__ void rev_levels(T (&s)[P0], T (&d)[P0],
         }
       }
       if constexpr (LV > 0)
-        rev_levels<T, WI, OP, P0, HMAX, LV - 1, TILE>(s, d, c);
+        rev_levels<T, VT, V, WI, OP, P0, HMAX, LV - 1, TILE>(s, d, c);
     } else if constexpr (LV > 0) {
-      rev_levels<T, WI, OP, P0, HMAX, LV - 1, TILE>(s, d, c);
+      rev_levels<T, VT, V, WI, OP, P0, HMAX, LV - 1, TILE>(s, d, c);
     }
   }
 }
@@ -412,9 +495,13 @@ constexpr int reg_max_levels(int wi, int op, int p0) {
   return lv;
 }
 
-template <typename T, int WI, int OP, int P0, bool STRIDED, bool TILE>
+// V: adjacent lines per lane (strided mode only; 2 packs float pairs into
+// FP32x2 arithmetic and 8-byte accesses).  lines per CTA = lpc * V.
+template <typename T, int WI, int OP, int P0, bool STRIDED, bool TILE, int V>
 __global__ void __launch_bounds__(512)
     reg_kernel(const __grid_constant__ RegParams<T> p) {
+  using VT = typename LaneVec<T, V>::type;
+  static_assert(V == 1 || STRIDED, "vector lanes need the strided mapping");
   constexpr int HMAX = cat_reach(WI, OP) > 0 ? cat_reach(WI, OP) : 1;
   constexpr bool FWD = (OP == TF_F || OP == TF_IA);
   extern __shared__ __align__(16) unsigned char lw_reg_smem[];
@@ -423,16 +510,18 @@ __global__ void __launch_bounds__(512)
   c.nth = blockDim.x;
   c.tid = threadIdx.x;
   c.mb = reinterpret_cast<T*>(lw_reg_smem);
-  c.cA = c.mb + 4 * HMAX * c.nth;
+  // mailbox: 4 * HMAX * nth lane values, then the coarse buffers
+  c.cA = reinterpret_cast<T*>(reinterpret_cast<VT*>(c.mb) + 4 * HMAX * c.nth);
   c.cA = reinterpret_cast<T*>(
       (reinterpret_cast<uintptr_t>(c.cA) + 15) & ~uintptr_t(15));
-  const int lines_cta = STRIDED ? 32 : p.lpc;
+  const int lpc = p.lpc;               // lanes (line groups) per CTA row
+  const int lines_cta = lpc * V;
   c.cB = c.cA + (int64_t)lines_cta * p.coarse_pitch;
   if (STRIDED) {
-    c.j = c.tid & 31;
-    c.r = c.tid >> 5;
-    c.tid_l = c.tid - 32;
-    c.tid_r = c.tid + 32;
+    c.j = c.tid % lpc;
+    c.r = c.tid / lpc;
+    c.tid_l = c.tid - lpc;
+    c.tid_r = c.tid + lpc;
   } else {
     c.j = c.tid / p.tpl;
     c.r = c.tid - c.j * p.tpl;
@@ -447,8 +536,8 @@ __global__ void __launch_bounds__(512)
     tile_idx = blockIdx.x % p.ntiles;
     group = blockIdx.x / p.ntiles;
   }
-  c.L = group * lines_cta + c.j;
-  c.line_ok = c.L < p.g.nlines;
+  c.L = group * lines_cta + (int64_t)c.j * V;
+  c.line_ok = c.L < p.g.nlines;  // V lines together (nlines % V == 0)
   c.bin = 0;
   c.bout = 0;
   if (c.line_ok) line_base(p.g, c.L, c.bin, c.bout);
@@ -463,21 +552,21 @@ __global__ void __launch_bounds__(512)
     c.tile_hi = c.n;
   }
 
-  T s[P0], d[P0];
+  VT s[P0], d[P0];
   if constexpr (FWD) {
     const bool in_band = c.line_ok && c.e0 >= 0 && c.e0 < c.n;
     const T* src = p.in + c.bin + c.e0 * p.g.sin;
     constexpr int VW = 16 / (int)sizeof(T);
-    if (in_band && p.vec && (c.e0 % VW) == 0) {
+    if (V == 1 && in_band && p.vec && (c.e0 % VW) == 0) {
 #pragma unroll
       for (int e = 0; e < 2 * P0; e += VW) {
-        if constexpr (sizeof(T) == 4) {
+        if constexpr (V == 1 && sizeof(T) == 4) {
           const float4 v = *reinterpret_cast<const float4*>(src + e);
           s[e / 2] = v.x;
           d[e / 2] = v.y;
           s[e / 2 + 1] = v.z;
           d[e / 2 + 1] = v.w;
-        } else {
+        } else if constexpr (V == 1) {
           const double2 v = *reinterpret_cast<const double2*>(src + e);
           s[e / 2] = v.x;
           d[e / 2] = v.y;
@@ -486,11 +575,13 @@ __global__ void __launch_bounds__(512)
     } else {
 #pragma unroll
       for (int i = 0; i < P0; ++i) {
-        s[i] = in_band ? src[(2 * i) * p.g.sin] : T(0);
-        d[i] = in_band ? src[(2 * i + 1) * p.g.sin] : T(0);
+        s[i] = in_band ? *reinterpret_cast<const VT*>(src + (2 * i) * p.g.sin)
+                       : vzero<VT>();
+        d[i] = in_band ? *reinterpret_cast<const VT*>(src + (2 * i + 1) * p.g.sin)
+                       : vzero<VT>();
       }
     }
-    reg::fwd_levels<T, WI, OP, P0, HMAX, 0, TILE>(s, d, c);
+    reg::fwd_levels<T, VT, V, WI, OP, P0, HMAX, 0, TILE>(s, d, c);
     if constexpr (!TILE) {
       if (p.nreg < p.levels) {
         __syncthreads();
@@ -548,7 +639,7 @@ __global__ void __launch_bounds__(512)
       }
     }
     constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
-    reg::rev_levels<T, WI, OP, P0, HMAX, TOP, TILE>(s, d, c);
+    reg::rev_levels<T, VT, V, WI, OP, P0, HMAX, TOP, TILE>(s, d, c);
   }
 }
 

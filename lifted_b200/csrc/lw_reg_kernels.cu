@@ -9,6 +9,7 @@
 
 #include "lw_launch.hpp"
 #include "lw_reg.hpp"
+#include "lw_reg_inst.hpp"
 #include "lw_reg_kernel.cuh"
 #include "lw_wrow.hpp"
 #include "lw_wrow_kernel.cuh"
@@ -28,56 +29,11 @@ constexpr int p0_of() {
 }
 
 template <typename T>
-using RegFn = cudaError_t (*)(const RegParams<T>&, int, int, size_t,
-                              cudaStream_t);
-
-template <typename T, int WI, int OP, bool STRIDED, bool TILE>
-cudaError_t launch_one(const RegParams<T>& p, int grid, int block, size_t smem,
-                       cudaStream_t stream) {
-  constexpr int P0 = p0_of<T>();
-  auto kern = reg_kernel<T, WI, OP, P0, STRIDED, TILE>;
-  static bool configured[kMaxDevices] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (!configured[dev]) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kMaxDynSmem);
-    if (e != cudaSuccess) return e;
-    configured[dev] = true;
-  }
-  kern<<<grid, block, smem, stream>>>(p);
-  return cudaGetLastError();
-}
-
-template <typename T, int WI, int OP>
-RegFn<T> pick_mode(bool strided, bool tile) {
-  if (strided)
-    return tile ? launch_one<T, WI, OP, true, true>
-                : launch_one<T, WI, OP, true, false>;
-  return tile ? launch_one<T, WI, OP, false, true>
-              : launch_one<T, WI, OP, false, false>;
-}
-
-template <typename T, int WI>
-RegFn<T> pick_op(int op, bool strided, bool tile) {
-  switch (op) {
-    case 0: return pick_mode<T, WI, 0>(strided, tile);
-    case 1: return pick_mode<T, WI, 1>(strided, tile);
-    case 2: return pick_mode<T, WI, 2>(strided, tile);
-    default: return pick_mode<T, WI, 3>(strided, tile);
-  }
-}
-
-template <typename T>
-RegFn<T> pick(int wi, int op, bool strided, bool tile) {
-  switch (wi) {
-    case WI_DB2: return pick_op<T, WI_DB2>(op, strided, tile);
-    case WI_DB4: return pick_op<T, WI_DB4>(op, strided, tile);
-    case WI_CDF97: return pick_op<T, WI_CDF97>(op, strided, tile);
-    default: return nullptr;
-  }
+RegFn<T> pick(int wi, int op, bool strided, bool tile, int v) {
+  if constexpr (sizeof(T) == 4)
+    return pick_reg_f32(wi, op, strided, tile, v);
+  else
+    return pick_reg_f64(wi, op, strided, tile, v);
 }
 
 bool compiled_wavelet(int wi) {
@@ -111,6 +67,20 @@ bool rows_vectorisable(const LineGeom& g, const T* in, const T* out) {
   return true;
 }
 
+// Two adjacent lines per lane (float only): even line count, even strides
+// and 8-byte aligned bases so every lane access is one aligned float2.
+template <typename T>
+int lane_width(const LineGeom& g, const T* in, const T* out) {
+  if (sizeof(T) != 4) return 1;
+  if (g.nlines % 2 || g.nother < 1 || (g.oshape[0] % 2)) return 1;
+  if ((g.sin % 2) || (g.sout % 2)) return 1;
+  for (int d = 1; d < g.nother; ++d)
+    if ((g.oin[d] % 2) || (g.oout[d] % 2)) return 1;
+  if ((reinterpret_cast<uintptr_t>(in) & 7) || (reinterpret_cast<uintptr_t>(out) & 7))
+    return 1;
+  return 2;
+}
+
 // Lines adjacent in memory along the fastest other dim (both sides).
 bool lines_adjacent(const LineGeom& g) {
   return g.nother >= 1 && g.oin[0] == 1 && g.oout[0] == 1;
@@ -118,8 +88,8 @@ bool lines_adjacent(const LineGeom& g) {
 
 template <typename T>
 size_t reg_smem(int hmax, int block, int lines_cta, int64_t m_coarse,
-                bool coarse) {
-  size_t b = (size_t)4 * hmax * block * sizeof(T) + 16;
+                bool coarse, int v = 1) {
+  size_t b = (size_t)4 * hmax * block * sizeof(T) * v + 16;
   if (coarse)  // A and B, each m elements per line (coarse_forward/_reverse)
     b += (size_t)lines_cta * (size_t)(2 * m_coarse) * sizeof(T);
   return b;
@@ -138,8 +108,11 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   const int nreg = levels < maxreg ? levels : maxreg;
   if (nreg < 1) return 0;
   int lpc = 1, block;
+  int v = 1;
   if (strided) {
     if (tpl > 16) return 0;
+    v = lane_width<T>(g, in, out);
+    lpc = 32;
     block = 32 * (int)tpl;
   } else {
     if (tpl > 512) return 0;
@@ -148,11 +121,11 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
     if (lpc > g.nlines) lpc = (int)g.nlines;
     block = lpc * (int)tpl;
   }
-  const int lines_cta = strided ? 32 : lpc;
+  const int lines_cta = lpc * v;
   const int64_t m = n >> nreg;
   const bool coarse = nreg < levels;
   const int hmax = cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1;
-  const size_t smem = reg_smem<T>(hmax, block, lines_cta, m, coarse);
+  const size_t smem = reg_smem<T>(hmax, block, lines_cta, m, coarse, v);
   if (smem > kMaxDynSmem) return 0;
   RegParams<T> p;
   std::memset(&p, 0, sizeof(p));
@@ -169,7 +142,7 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   p.prog = *a.prog;
   const int64_t groups = (g.nlines + lines_cta - 1) / lines_cta;
   if (groups > 0x7fffffffLL) return 0;
-  RegFn<T> fn = pick<T>(wi, op, strided, false);
+  RegFn<T> fn = pick<T>(wi, op, strided, false, v);
   if (!fn) return 0;
   cudaError_t e = fn(p, (int)groups, block, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
@@ -248,9 +221,10 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   const int tpl = (int)(ichunks + 2 * hchunks);
   const int block = 32 * tpl;
   const int hmax = cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1;
-  const size_t smem = reg_smem<T>(hmax, block, 32, 0, false);
+  const int v = lane_width<T>(g, a.in, a.out);
+  const size_t smem = reg_smem<T>(hmax, block, 32 * v, 0, false, v);
   const int64_t ntiles = (n + tile - 1) / tile;
-  const int64_t groups = (g.nlines + 31) / 32;
+  const int64_t groups = (g.nlines + 32 * v - 1) / (32 * v);
   if (groups * ntiles > 0x7fffffffLL) return 0;
   // the whole-line launch on the approximation band must be possible too
   if (a.levels > k && ((m % (2 * P0)) || (m / (2 * P0)) > 16)) return 0;
@@ -277,7 +251,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   p.halo = halo;
   p.ntiles = ntiles;
   p.prog = *a.prog;
-  RegFn<T> tfn = pick<T>(wi, op, true, true);
+  RegFn<T> tfn = pick<T>(wi, op, true, true, v);
   if (!tfn) {
     if (tmp) scratch_free(tmp, stream);
     return 0;
