@@ -184,8 +184,12 @@ __device__ __forceinline__ double2 vsub(double2 a, double2 b) {
 }
 __device__ __forceinline__ float vmul(float a, float b) { return a * b; }
 __device__ __forceinline__ double vmul(double a, double b) { return a * b; }
+// Scale multiplies stay two scalar __fmul_rn: the packed multiply may be
+// contracted with a following packed add (a unit step right after the scale
+// of a reverse-stepping program) into one fused operation, which rounds
+// differently from the reference's separate multiply and add.
 __device__ __forceinline__ float2 vmul(float2 a, float b) {
-  return __fmul2_rn(a, make_float2(b, b));
+  return make_float2(__fmul_rn(a.x, b), __fmul_rn(a.y, b));
 }
 __device__ __forceinline__ double2 vmul(double2 a, double b) {
   return make_double2(a.x * b, a.y * b);
