@@ -207,6 +207,180 @@ def run_reference_arm(args, rank: int) -> int:
     return 0
 
 
+def batched_section(dev, plain_sample: int = 300, steps: int = 5):
+    """Batched uneven 1D: 10,000 float32 signals, lengths round(2^U[8,20]),
+    wavelet uniform over the catalogue, levels U{1..max_level} (Lazy:
+    floor(log2 len)), Zero boundary; one step = Forward + ForwardAdjoint of
+    the whole batch, each one persistent launch replayed from a CUDA graph.
+    The plain per-call form (one C ABI call per signal and transform) is
+    timed on a seeded random sample of the same signals."""
+    import torch
+    from lifted_b200 import _lib
+    from lifted_b200 import pylifted as pl
+    from lifted_b200.batch import BatchPlan
+
+    rng = np.random.default_rng(1004)
+    n = 10000
+    lengths = np.round(2.0 ** rng.uniform(8, 20, n)).astype(np.int64)
+    values = _lib.wavelet_values()
+    ws = [values[i] for i in rng.integers(0, len(values), n)]
+    lv = []
+    for L, w in zip(lengths, ws):
+        width = _lib.wavelet_width(w)
+        mx = int(np.floor(np.log2(L))) if width == 1 else _lib.max_level(width, int(L))
+        lv.append(int(rng.integers(1, max(mx, 1) + 1)))
+    tot = int(lengths.sum())
+    g = torch.Generator(device=dev).manual_seed(1004)
+    x = torch.randn(tot, device=dev, generator=g)
+    y = torch.empty_like(x)
+    z = torch.empty_like(x)
+    pf = BatchPlan(lengths, ws, lv, op=0, dtype="float32")
+    pa = BatchPlan(lengths, ws, lv, op=2, dtype="float32")
+    for _ in range(3):
+        pf.run(x, out=y, graph=True)
+        pa.run(y, out=z, graph=True)
+    pf.check()
+    pa.check()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        pf.run(x, out=y, graph=True)
+        pa.run(y, out=z, graph=True)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    pf.check()
+    pa.check()
+    ms = e0.elapsed_time(e1) / steps
+    bytes_step = 2 * 2 * tot * 4
+    info = pf.info
+    # plain per-call form on a sample
+    idx = np.sort(rng.choice(n, size=min(plain_sample, n), replace=False))
+    offs = np.concatenate([[0], np.cumsum(lengths)[:-1]])
+    samp = int(lengths[idx].sum())
+
+    def plain():
+        for i in idx:
+            o, L = int(offs[i]), int(lengths[i])
+            pl._lwt(x[o:o + L], int(ws[i]), 0, 0, (0,), (lv[i],), 1, out=y[o:o + L])
+            pl._lwt(y[o:o + L], int(ws[i]), 0, 2, (0,), (lv[i],), 1, out=z[o:o + L])
+
+    plain()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    plain()
+    torch.cuda.synchronize(dev)
+    pel = time.perf_counter() - t0
+    plain_gbs = 2 * 2 * samp * 4 / pel / 1e9
+    pf.close()
+    pa.close()
+    gbs = bytes_step / ms / 1e6
+    return {"workload": "10,000 float32 signals, lengths round(2^U[8,20]) (seed 1004), "
+                        "wavelet uniform over the 34 catalogue wavelets, levels "
+                        "U{1..max_level}, Zero boundary, Forward + ForwardAdjoint",
+            "value": round(gbs, 3), "unit": "GB/s", "ms_per_step": round(ms, 4),
+            "samples": tot, "algorithmic_bytes_per_step": bytes_step,
+            "launches_per_step": 2, "cuda_graph": True,
+            "items": info["nitems"], "tiles": info["ntiles"],
+            "plain_per_call": {"value": round(plain_gbs, 3), "unit": "GB/s",
+                               "sample": f"{len(idx)} random signals of the batch "
+                                         f"({samp} samples), one C ABI call per signal "
+                                         f"and transform, wall clock"},
+            "speedup_vs_plain": round(gbs / plain_gbs, 1)}
+
+
+def autograd_section(dev, steps: int = 10):
+    """3D float32 512^3 (N(0,1) smoothed by an edge-clamped 3-point box per
+    axis), Daubechies4, levels (4,4,4) on axes (0,1,2), through the
+    torch.autograd.Function: forward, backward (the adjoint kernel), and the
+    plain pylifted forward for comparison."""
+    import torch
+    from lifted_b200 import autograd as ag
+    from lifted_b200 import pylifted as pl
+
+    g = torch.Generator(device=dev).manual_seed(1003)
+    v = torch.randn(512, 512, 512, device=dev, generator=g)
+    for ax in range(3):
+        p = torch.cat([v.narrow(ax, 0, 1), v, v.narrow(ax, 511, 1)], dim=ax)
+        v = (p.narrow(ax, 0, 512) + p.narrow(ax, 1, 512) + p.narrow(ax, 2, 512)) / 3
+    v = v.contiguous()
+    gy = torch.randn(512, 512, 512, device=dev, generator=g)
+    xr = v.clone().requires_grad_(True)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    fw, bw, plain = [], [], []
+    for k in range(steps + 2):
+        a, b, c, d, e = ev(), ev(), ev(), ev(), ev()
+        xr.grad = None
+        a.record()
+        yv = ag.dwt(xr, "db4", "Zero", axes=(0, 1, 2), level=(4, 4, 4))
+        b.record()
+        yv.backward(gy)
+        c.record()
+        pl.lwt_forward(v, "db4", "Zero", axes=(0, 1, 2), level=(4, 4, 4))
+        d.record()
+        torch.cuda.synchronize(dev)
+        if k >= 2:
+            fw.append(a.elapsed_time(b))
+            bw.append(b.elapsed_time(c))
+            plain.append(c.elapsed_time(d))
+    f, bk, pln = float(np.median(fw)), float(np.median(bw)), float(np.median(plain))
+    B = 2 * v.numel() * 4
+    return {"workload": "3D float32 512^3 box-smoothed N(0,1) (seed 1003), Daubechies4, "
+                        "levels (4,4,4), axes (0,1,2), Zero boundary",
+            "forward_ms": round(f, 4), "backward_ms": round(bk, 4),
+            "plain_forward_ms": round(pln, 4),
+            "backward_over_forward": round(bk / f, 3),
+            "forward_gbs": round(B / f / 1e6, 1), "backward_gbs": round(B / bk / 1e6, 1)}
+
+
+def lsq_section(dev, steps: int = 200, check_steps: int = 3):
+    """Wavelet-regularised least squares: 16 float32 2048^2 images,
+    0.5||Ax-b||^2 + lam||Wx||_1, A a seeded 5x5 blur, W CDF 9/7 5 levels
+    on the image axes, 200 gradient steps through the autograd DWT.  The
+    loss of image 0 over the first steps is checked against a float64 CPU
+    run of the same iteration with the oracle's transforms."""
+    import torch
+    from lifted_b200 import lsq
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    lam, eta = 0.01, 1.0
+    xt, b, k = lsq.make_problem(16, 2048, seed=1005)
+    loop = lsq.GradientLoop(b, k, lam, eta, levels=(5, 5), device=dev)
+    for _ in range(2):
+        loop.step()
+    loop.x.data.zero_()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = [loop.step() for _ in range(steps)]
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    first, last = float(losses[0]), float(losses[-1])
+    # float64 CPU check of image 0
+    loop0 = lsq.GradientLoop(b[:1], k, lam, eta, levels=(5, 5), device=dev)
+    g_loss, c_loss = [], []
+    x = np.zeros_like(b[0])
+    for _ in range(check_steps):
+        g_loss.append(float(loop0.step()))
+        r = lsq.blur_np(x, k) - b[0]
+        rc, wx = po.oracle_sep(x, 100907, 0, 0, [0, 1], [5, 5])
+        c_loss.append(0.5 * float(np.sum(r * r)) + lam * float(np.sum(np.abs(wx))))
+        rc2, wts = po.oracle_sep(np.sign(wx), 100907, 2, 0, [0, 1], [5, 5])
+        x = x - eta * (lsq.blur_adj_np(r, k) + lam * wts)
+    rel = max(abs(a - c) / abs(c) for a, c in zip(g_loss, c_loss))
+    return {"workload": "16 x 2048^2 float32, 0.5||Ax-b||^2 + 0.01||Wx||_1, 5x5 blur, "
+                        "CDF 9/7 levels (5,5), step 1.0, 200 gradient steps (seed 1005)",
+            "ms_per_step": round(ms, 4), "loss_first": first, "loss_last": last,
+            "image0_loss_vs_fp64_cpu_max_rel": rel,
+            "image0_checked_steps": check_steps}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,6 +389,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched, autograd and least-squares sections")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -339,6 +515,12 @@ def main() -> int:
                              f"(reference sources + Highway stand-in, {variant}, "
                              f"{cores} threads)"}
 
+    extras = {"batched": None, "autograd": None, "lsq": None}
+    if world == 1 and not args.no_extras:
+        extras["batched"] = batched_section(dev)
+        extras["autograd"] = autograd_section(dev)
+        extras["lsq"] = lsq_section(dev)
+
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -361,6 +543,9 @@ def main() -> int:
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "batched": extras["batched"],
+            "autograd": extras["autograd"],
+            "lsq": extras["lsq"],
         }
         print(json.dumps(line))
     if world > 1:

@@ -163,6 +163,105 @@ LIFTED_CAPI int lifted_lwt_sep_noalloc_f32(
     const ptrdiff_t* stride_out, size_t naxes, const size_t* axes,
     const size_t* levels, const float* in, float* out, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched uneven-length 1D transforms.
+ *
+ * The reference transforms one array per call (lifted::lwt,
+ * src/lifted.hpp:13-39); a batch of signals of different lengths, wavelets
+ * and level counts is a loop of such calls (src/pylifted/_wavelets.pyx:
+ * 185-276 per call).  Here a batch is one persistent kernel launch that pulls
+ * work items (a whole signal, or a tile of a long signal's band over a group
+ * of levels) from a device queue.  Each signal's result is that of the
+ * separable transform of the 1D array alone:
+ *     lifted_lwt_sep_xxx(wavelet, op, bc, 1, {length}, {1}, {1}, 1, {0},
+ *                        {levels}, in + in_offset, out + out_offset, stream)
+ * Signals are contiguous (unit stride) in `in` and `out`, which must be
+ * device (or managed) memory and must not overlap each other.  Signals may
+ * share input but their output ranges must be disjoint. */
+typedef struct lifted_signal {
+  uint32_t wavelet;     /* lifted::Wavelet value */
+  uint32_t levels;      /* levels; 0 = max_level(width, length) */
+  uint64_t length;      /* samples (0: the signal is skipped) */
+  uint64_t in_offset;   /* element offset of the signal in `in` */
+  uint64_t out_offset;  /* element offset of its result in `out` */
+} lifted_signal_t;
+
+/* Optional planner settings (0 = default or autotuned):
+ *   block        threads per CTA of the persistent kernel (64..512)
+ *   whole_max    longest band transformed as one whole item in shared
+ *                memory (default 4096 float32, 2048 float64)
+ *   tile         interior width of a tile item, samples of its band
+ *   tile_levels  levels per tile group (Zero boundary only) */
+typedef struct lifted_batch_tuning {
+  uint32_t block;
+  uint32_t whole_max;
+  uint32_t tile;
+  uint32_t tile_levels;
+} lifted_batch_tuning_t;
+
+typedef struct lifted_batch_info {
+  uint64_t nsignals, nitems, ntiles, nwhole, nwhole_global, ncounters;
+  uint64_t scratch_bytes, shared_bytes;
+  uint32_t grid, block;
+} lifted_batch_info_t;
+
+typedef struct lifted_batch_plan lifted_batch_plan_t;
+
+/* Plans a batch: validates every signal (as the separable entry would),
+ * resolves its levels, cuts it into work items, allocates the plan's device
+ * buffers (work queue, programs, completion counters, scratch bands).  Tile
+ * width and levels per tile group come from `tuning`, else from the
+ * autotuner's table for (wavelet, dtype, transform, length), else from a
+ * halo-based default. */
+LIFTED_CAPI int lifted_batch_plan_create_f32(uint32_t op, uint32_t bc, size_t nsignals,
+                                             const lifted_signal_t* signals,
+                                             const lifted_batch_tuning_t* tuning,
+                                             lifted_batch_plan_t** plan);
+LIFTED_CAPI int lifted_batch_plan_create_f64(uint32_t op, uint32_t bc, size_t nsignals,
+                                             const lifted_signal_t* signals,
+                                             const lifted_batch_tuning_t* tuning,
+                                             lifted_batch_plan_t** plan);
+/* Enqueues one run on `stream` (a memset of the queue counters and one
+ * kernel launch; stream-ordered, no synchronisation, may be captured into a
+ * CUDA graph).  Runs of one plan must not overlap on the GPU. */
+LIFTED_CAPI int lifted_batch_run(lifted_batch_plan_t* plan, const void* in, void* out,
+                                 void* stream);
+/* As lifted_batch_run, replayed from a CUDA graph the plan captures on first
+ * use (and again whenever `in` or `out` change). */
+LIFTED_CAPI int lifted_batch_run_graph(lifted_batch_plan_t* plan, const void* in, void* out,
+                                       void* stream);
+/* Synchronises `stream` and reports LIFTED_ETIMEOUT if an item of the last
+ * run gave up waiting (bounded) for the band another item produces. */
+LIFTED_CAPI int lifted_batch_check(lifted_batch_plan_t* plan, void* stream);
+LIFTED_CAPI int lifted_batch_plan_info(const lifted_batch_plan_t* plan,
+                                       lifted_batch_info_t* info);
+/* Fields of work item `index` in queue order: kind, program, signal, lev0,
+ * nlev, src_sel, dst_sel, wait_ctr, wait_target, done_ctr, n0, in_off,
+ * out_off, src_off, dst_off, t0, t1, halo, gbuf, phase (for tests and
+ * diagnostics). */
+LIFTED_CAPI int lifted_batch_plan_item(const lifted_batch_plan_t* plan, size_t index,
+                                       int64_t* fields, size_t nfields);
+LIFTED_CAPI void lifted_batch_plan_destroy(lifted_batch_plan_t* plan);
+/* One-shot: plan, run, check, destroy (synchronous). */
+LIFTED_CAPI int lifted_lwt_batch_f32(uint32_t op, uint32_t bc, size_t nsignals,
+                                     const lifted_signal_t* signals, const float* in,
+                                     float* out, void* stream);
+LIFTED_CAPI int lifted_lwt_batch_f64(uint32_t op, uint32_t bc, size_t nsignals,
+                                     const lifted_signal_t* signals, const double* in,
+                                     double* out, void* stream);
+/* Autotuner: for each wavelet, times every (tile width, levels per tile
+ * group) candidate on a synthetic batch of `total` samples cut into signals
+ * of `length`, and records the fastest in the process-wide table keyed by
+ * (wavelet, dtype, transform, log2 length, stride 1) that later plans
+ * consult.  Allocates its own device buffers. */
+LIFTED_CAPI int lifted_batch_autotune(uint32_t dtype_bytes, uint32_t op, uint32_t bc,
+                                      size_t nwavelets, const uint32_t* wavelets,
+                                      size_t length, size_t total, void* stream);
+/* The tuning table as JSON (one entry per line), and back. */
+LIFTED_CAPI int lifted_batch_tune_save(const char* path);
+LIFTED_CAPI int lifted_batch_tune_load(const char* path, size_t* loaded);
+LIFTED_CAPI void lifted_batch_tune_clear(void);
+
 /* max_level(width, n) of the reference (src/lifted-common.hpp:1099-1108);
  * returns (size_t)-1 for width 1, where the reference never returns. */
 LIFTED_CAPI size_t lifted_max_level(size_t width, size_t n);

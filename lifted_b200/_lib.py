@@ -49,6 +49,38 @@ class Step(ctypes.Structure):
     ]
 
 
+class Signal(ctypes.Structure):
+    """lifted_signal_t."""
+
+    _fields_ = [
+        ("wavelet", ctypes.c_uint32),
+        ("levels", ctypes.c_uint32),
+        ("length", ctypes.c_uint64),
+        ("in_offset", ctypes.c_uint64),
+        ("out_offset", ctypes.c_uint64),
+    ]
+
+
+class BatchTuning(ctypes.Structure):
+    """lifted_batch_tuning_t."""
+
+    _fields_ = [
+        ("block", ctypes.c_uint32),
+        ("whole_max", ctypes.c_uint32),
+        ("tile", ctypes.c_uint32),
+        ("tile_levels", ctypes.c_uint32),
+    ]
+
+
+class BatchInfo(ctypes.Structure):
+    """lifted_batch_info_t."""
+
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "nsignals", "nitems", "ntiles", "nwhole", "nwhole_global", "ncounters",
+        "scratch_bytes", "shared_bytes")] + [("grid", ctypes.c_uint32),
+                                              ("block", ctypes.c_uint32)]
+
+
 _lock = threading.Lock()
 _lib = None
 
@@ -63,6 +95,20 @@ for _suf in ("f32", "f64"):
     _SIGS[f"lifted_lwt_{_suf}"] = (ctypes.c_int, [_u32, _u32, _u32, _sz, _p, _p, _p, _sz, _p, _sz, _p, _p, _p])
     _SIGS[f"lifted_lwt_sep_program_{_suf}"] = (ctypes.c_int, [_p, _sz, _sz, _u32, _u32, _sz, _p, _p, _p, _sz, _p, _p, _p, _p, _p])
 _SIGS["lifted_lwt_sep_noalloc_f32"] = (ctypes.c_int, [_u32, _u32, _u32, _sz, _p, _p, _p, _sz, _p, _p, _p, _p, _p])
+_SIGS["lifted_batch_plan_create_f32"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p])
+_SIGS["lifted_batch_plan_create_f64"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p])
+_SIGS["lifted_batch_run"] = (ctypes.c_int, [_p, _p, _p, _p])
+_SIGS["lifted_batch_run_graph"] = (ctypes.c_int, [_p, _p, _p, _p])
+_SIGS["lifted_batch_check"] = (ctypes.c_int, [_p, _p])
+_SIGS["lifted_batch_plan_info"] = (ctypes.c_int, [_p, _p])
+_SIGS["lifted_batch_plan_item"] = (ctypes.c_int, [_p, _sz, _p, _sz])
+_SIGS["lifted_batch_plan_destroy"] = (None, [_p])
+_SIGS["lifted_lwt_batch_f32"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
+_SIGS["lifted_lwt_batch_f64"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
+_SIGS["lifted_batch_autotune"] = (ctypes.c_int, [_u32, _u32, _u32, _sz, _p, _sz, _sz, _p])
+_SIGS["lifted_batch_tune_save"] = (ctypes.c_int, [ctypes.c_char_p])
+_SIGS["lifted_batch_tune_load"] = (ctypes.c_int, [ctypes.c_char_p, _p])
+_SIGS["lifted_batch_tune_clear"] = (None, [])
 _SIGS["lifted_max_level"] = (_sz, [_sz, _sz])
 _SIGS["lifted_wavelet_width"] = (_sz, [_u32])
 _SIGS["lifted_wavelet_count"] = (_sz, [])

@@ -335,6 +335,8 @@ bool dense(size_t ndim, const size_t* shape, const ptrdiff_t* stride) {
 
 }  // namespace
 
+bool device_pointer(const void* p) { return is_device_pointer(p); }
+
 // ---------------------------------------------------------------------------
 // Axis passes.
 namespace {

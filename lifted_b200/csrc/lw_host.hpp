@@ -51,6 +51,8 @@ void resolve_program(const Program& prog, int op, int across,
                      DevProgram<T>* out);
 
 size_t max_level(size_t width, size_t n);
+// Device or managed memory (cudaPointerGetAttributes).
+bool device_pointer(const void* p);
 bool line_degenerate(const Program& prog, int op, int bc, int64_t n,
                      size_t levels);
 size_t wavelet_count();

@@ -1,0 +1,123 @@
+"""Batch planner on the CPU: the work items of lifted_batch plans, executed
+in queue order by the CPU emulator (tests/batch_emulator.py), reproduce the
+oracle's transform of every signal alone, bit for bit; the queue puts every
+producer group before its consumers; invalid batches are refused like the
+separable entry refuses the same signal.  No GPU needed: a plan touches the
+device only on its first run."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from batch_emulator import emulate, prog_wavelets
+from lifted_b200 import _lib
+from lifted_b200.batch import ITEM_FIELDS, KIND_NAMES, BatchPlan
+
+# Daubechies2/4/10, Coiflet3, Bior3_9, CDF5_3, CDF9_7, Lazy, Symlet6, Bior6_8
+WAVELETS = [2, 4, 10, 203, 10309, 100503, 100907, 0, 106, 10608]
+
+
+def make_batch(seed, n, maxlen, dtype, levels_mode="random"):
+    rng = np.random.default_rng(seed)
+    lengths = rng.integers(1, maxlen, n)
+    ws = [WAVELETS[i] for i in rng.integers(0, len(WAVELETS), n)]
+    lv = []
+    for L, w in zip(lengths, ws):
+        width = po.wavelet_width(w)
+        mx = int(np.floor(np.log2(L))) if width == 1 else po.max_level(width, int(L))
+        mx = max(mx, 1)
+        lv.append(int(rng.integers(1, mx + 1)) if levels_mode == "random" else mx)
+    x = rng.standard_normal(int(lengths.sum())).astype(dtype)
+    return lengths, ws, lv, x
+
+
+def oracle_batch(x, lengths, ws, lv, op, bc):
+    out = np.zeros_like(x)
+    off = 0
+    for L, w, l in zip(lengths, ws, lv):
+        sig = x[off:off + L].copy()
+        rc, o = po.oracle_sep(sig, w, op, bc, [0], [l])
+        if rc == 0:
+            out[off:off + L] = o
+        off += L
+    return out
+
+
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_emulated_tiles_match_oracle(op, dtype):
+    lengths, ws, lv, x = make_batch(100 + op, 40, 3000, dtype)
+    # small whole items and tiles force multi-group tiling on modest lengths
+    for tuning in ({"whole_max": 256, "tile": 128},
+                   {"whole_max": 200, "tile": 512, "tile_levels": 3},
+                   {"whole_max": 64, "tile": 64, "tile_levels": 1}):
+        plan = BatchPlan(lengths, ws, lv, op=op, mode="Zero", dtype=dtype, tuning=tuning)
+        items = plan.items()
+        info = plan.info
+        assert info["ntiles"] > 0
+        got, _ = emulate(items, op, 0, prog_wavelets(ws), x, plan.out_elems,
+                         info["scratch_bytes"] // x.itemsize)
+        want = oracle_batch(x, lengths, ws, lv, op, 0)
+        assert np.array_equal(got[:len(want)], want), tuning
+        plan.close()
+
+
+@pytest.mark.parametrize("bc", [1, 2, 3, 4])
+def test_other_boundaries_run_whole_items(bc):
+    lengths, ws, lv, x = make_batch(7 + bc, 25, 1500, np.float64)
+    plan = BatchPlan(lengths, ws, lv, op=2, mode=bc, dtype="float64",
+                     tuning={"whole_max": 256})
+    items = plan.items()
+    kinds = {KIND_NAMES[k] for k in items[:, 0]}
+    assert kinds <= {"whole_fwd", "whole_rev"}
+    # bands beyond whole_max get global buffers
+    assert plan.info["nwhole_global"] == int(np.sum(np.asarray(lengths) > 256))
+    got, _ = emulate(items, 2, bc, prog_wavelets(ws), x, plan.out_elems,
+                     plan.info["scratch_bytes"] // 8)
+    want = oracle_batch(x, lengths, ws, lv, 2, bc)
+    assert np.array_equal(got[:len(want)], want)
+
+
+def test_queue_order_and_counters():
+    lengths, ws, lv, x = make_batch(5, 60, 20000, np.float32, levels_mode="max")
+    for op in (0, 2):
+        plan = BatchPlan(lengths, ws, lv, op=op, dtype="float32",
+                         tuning={"whole_max": 512, "tile": 1024})
+        items = plan.items()
+        f = {k: i for i, k in enumerate(ITEM_FIELDS)}
+        produced = {}
+        for row in items:
+            if row[f["done_ctr"]] >= 0:
+                produced[row[f["done_ctr"]]] = produced.get(row[f["done_ctr"]], 0) + 1
+        seen = {}
+        for row in items:
+            if row[f["wait_ctr"]] >= 0:
+                c = row[f["wait_ctr"]]
+                # every producer of c is earlier in the queue
+                assert seen.get(c, 0) == produced[c] == row[f["wait_target"]]
+            if row[f["done_ctr"]] >= 0:
+                seen[row[f["done_ctr"]]] = seen.get(row[f["done_ctr"]], 0) + 1
+        # tiles are aligned to their level group
+        for row in items:
+            if KIND_NAMES[row[f["kind"]]].startswith("tile"):
+                a = 1 << int(row[f["nlev"]])
+                assert row[f["t0"]] % a == 0 and row[f["halo"]] % a == 0
+        # phases never decrease along the queue
+        assert np.all(np.diff(items[:, f["phase"]]) >= 0)
+        plan.close()
+
+
+def test_invalid_batches_refused():
+    with pytest.raises(KeyError):
+        BatchPlan([100], [12345], [1])          # unknown wavelet (pylifted's error)
+    with pytest.raises(_lib.LiftedValueError):
+        BatchPlan([100], [0], [0])              # Lazy with level 0 (Q14)
+    with pytest.raises(_lib.LiftedValueError):
+        BatchPlan([100], [2], [64])             # more than MAX_LEVELS
+    with pytest.raises(_lib.LiftedValueError):
+        BatchPlan([1], [2], [3], mode="Reflect")  # Reflect on a one-element band
+    with pytest.raises(_lib.LiftedValueError):
+        BatchPlan([100], [2], [1], tuning={"block": 100})
+    # zero-length signals and zero resolved levels are no-ops
+    p = BatchPlan([0, 3], [2, 4], [1, 0])
+    assert p.info["nitems"] == 0
+    p.close()
