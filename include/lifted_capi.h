@@ -280,8 +280,14 @@ LIFTED_CAPI uint64_t lifted_launch_count(void);
 /* Process-wide tuning/testing knobs:
  *   "force_global_scratch" 0/1  keep line buffers in global scratch even
  *                               when a line fits in shared memory
- *   "max_global_ctas"      n    CTAs of the global-scratch line path */
+ *   "max_global_ctas"      n    CTAs of the global-scratch line path
+ *   "fast_path"            0/1  register-blocked kernels where they apply
+ *   "tma_strided"          0/1  TMA-staged kernel for strided float32 passes */
 LIFTED_CAPI int lifted_set_option(const char* name, int64_t value);
+/* Synchronises `stream` and reports LIFTED_ETIMEOUT if a kernel of this
+ * library gave up a bounded device-side wait since the last check (the
+ * affected output is not valid).  Clears the condition. */
+LIFTED_CAPI int lifted_device_check(void* stream);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,7 @@ std::atomic<uint64_t> g_launches{0};
 std::atomic<int64_t> g_opt_force_global{0};
 std::atomic<int64_t> g_opt_max_global_ctas{296};
 std::atomic<int64_t> g_opt_fast_path{1};
+std::atomic<int64_t> g_opt_tma_strided{1};
 
 }  // namespace
 
@@ -793,6 +794,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_force_global = value ? 1 : 0;
   } else if (!std::strcmp(name, "fast_path")) {
     g_opt_fast_path = value ? 1 : 0;
+  } else if (!std::strcmp(name, "tma_strided")) {
+    g_opt_tma_strided = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");
@@ -803,6 +806,7 @@ int set_option(const char* name, int64_t value) {
   return LIFTED_OK;
 }
 uint64_t launch_count() { return g_launches.load(); }
+bool col_enabled() { return g_opt_tma_strided.load() != 0; }
 
 }  // namespace lw
 
@@ -891,6 +895,15 @@ LIFTED_CAPI const char* lifted_status_string(int status) {
 }
 LIFTED_CAPI const char* lifted_last_error(void) { return lw::last_error(); }
 LIFTED_CAPI uint64_t lifted_launch_count(void) { return lw::launch_count(); }
+LIFTED_CAPI int lifted_device_check(void* stream) {
+  lw::clear_error();
+  const int v = lw::check_col_errors((cudaStream_t)stream);
+  if (v < 0) return lw::set_error(LIFTED_ECUDA, "device status check failed");
+  if (v > 0)
+    return lw::set_error(LIFTED_ETIMEOUT,
+                         "a strided-pass kernel gave up waiting for a staging copy");
+  return LIFTED_OK;
+}
 LIFTED_CAPI int lifted_set_option(const char* name, int64_t value) {
   lw::clear_error();
   return lw::set_option(name, value);

@@ -30,4 +30,12 @@ struct RegStats {
 template <typename T>
 int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats);
 
+// Whether strided float32 passes may use the TMA-staged kernel (the
+// "tma_strided" option; on by default).
+bool col_enabled();
+// Synchronises `stream`; returns 1 (and clears it) if a TMA-staged kernel
+// gave up waiting for a staging copy since the last check, 0 if not, -1 if
+// the check itself failed.
+int check_col_errors(cudaStream_t stream);
+
 }  // namespace lw

@@ -4,9 +4,14 @@
 // general line kernel.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
+#include <cuda.h>
+
+#include "lw_col.hpp"
+#include "lw_col_kernel.cuh"
 #include "lw_launch.hpp"
 #include "lw_reg.hpp"
 #include "lw_reg_inst.hpp"
@@ -55,6 +60,24 @@ bool structure_matches(const DevProgram<T>& prog, int wi, int op) {
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+int sm_count() {
+  static int n[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return 148;
+  }
+  if (!n[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+      cudaGetLastError();
+      v = 148;
+    }
+    n[dev] = v;
+  }
+  return n[dev];
+}
 
 // Unit-stride rows whose line bases are all 16-byte aligned.
 template <typename T>
@@ -113,7 +136,11 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
     if (tpl > 16) return 0;
     v = lane_width<T>(g, in, out);
     lpc = 32;
-    block = 32 * (int)tpl;
+    // short bands of few lines: narrower line groups keep every SM busy
+    const int64_t want = (int64_t)sm_count();
+    if ((g.nlines + 63) / 64 < want) v = 1;
+    while (lpc > 8 && (g.nlines + lpc * v - 1) / (lpc * v) < want) lpc /= 2;
+    block = lpc * (int)tpl;
   } else {
     if (tpl > 512) return 0;
     lpc = (int)(256 / tpl);
@@ -309,7 +336,192 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   return rc;
 }
 
+// Device word the TMA-staged kernel sets when a staging wait gives up.
+int32_t* col_error_flag() {
+  static int32_t* flag[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  if (!flag[dev]) {
+    if (cudaMalloc((void**)&flag[dev], sizeof(int32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    cudaMemset(flag[dev], 0, sizeof(int32_t));
+  }
+  return flag[dev];
+}
+
+bool encode_rows(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims,
+                 const cuuint64_t* strides, cuuint32_t box_y) {
+  const cuuint32_t box[3] = {(cuuint32_t)COL_LANES, box_y, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return cuTensorMapEncodeTiled(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank,
+                                const_cast<void*>(base), dims, strides, box, es,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Strided float32 pass on the TMA-staged persistent kernel: whole lines of
+// up to 512 samples, or 512-sample windows with halos on longer lines; the
+// levels beyond the first k run as a strided whole-line launch on the
+// approximation band.  Returns 0 when the pass does not qualify.
+template <typename T>
+int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
+  if constexpr (sizeof(T) != 4) {
+    return 0;
+  } else {
+    const LineGeom& g = a.g;
+    if (!col_enabled()) return 0;
+    if (g.sin <= 1 || ((g.sin * 4) & 15)) return 0;
+    if (!lines_adjacent(g) || g.nother > 2) return 0;
+    const int64_t ncols = g.oshape[0];
+    if (ncols % COL_LANES) return 0;
+    if (g.nother == 2 && (g.oin[1] <= 0 || ((g.oin[1] * 4) & 15))) return 0;
+    if (!aligned16(a.in)) return 0;
+    const int64_t n = g.n;
+    if (n % 32) return 0;
+    const int wi = a.wi, op = a.op;
+    ColFn fn = pick_col(wi, op);
+    if (!fn) return 0;
+    const int maxreg = std::min(reg_max_levels(wi, op, COL_P0), COL_MAXK);
+    int k = 0;
+    int64_t tile, halo, ntr;
+    if (n <= COL_ROWS) {
+      k = std::min(a.levels, maxreg);
+      tile = n;
+      halo = 0;
+      ntr = 1;
+    } else {
+      if (a.in_place) return 0;  // windows would overwrite other windows' input
+      for (int kk = 1; kk <= maxreg && kk <= a.levels; ++kk) {
+        k = kk;
+        const int64_t m = n >> kk;
+        if (m % 32 == 0 && m / 32 <= 16) break;
+      }
+      int64_t need = 0;
+      const int lh = cat_level_halo(wi, op);
+      for (int l = 1; l <= k; ++l) need += (int64_t)lh << l;
+      halo = (need + 31) / 32 * 32;
+      tile = COL_ROWS - 2 * halo;
+      if (tile < 128) return 0;
+      ntr = (n + tile - 1) / tile;
+    }
+    if (k < 1) return 0;
+    const int64_t m = n >> k;
+    const bool more = a.levels > k;
+    if (more && ((m % 32) || m / 32 > 16)) return 0;
+    if (!more && a.levels != k) return 0;
+    int32_t* err = col_error_flag();
+    if (!err) return 0;
+
+    T* tmp = nullptr;
+    if (more) {
+      cudaError_t e = scratch_alloc((void**)&tmp, (size_t)g.nlines * m * sizeof(T), stream);
+      if (e != cudaSuccess) return -(int)e - 1000;
+    }
+    ColParams cp;
+    std::memset(&cp, 0, sizeof(cp));
+    const int rank = g.nother == 2 ? 3 : 2;
+    const cuuint64_t dims[3] = {(cuuint64_t)ncols, (cuuint64_t)n,
+                                (cuuint64_t)(g.nother == 2 ? g.oshape[1] : 1)};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.sin * 4,
+                                   (cuuint64_t)(g.nother == 2 ? g.oin[1] : 0) * 4};
+    bool ok = true;
+    for (int i = 0; i < k && ok; ++i)
+      ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, (cuuint32_t)(256 >> i));
+    if (ok && more) {
+      const cuuint64_t tdims[2] = {(cuuint64_t)g.nlines, (cuuint64_t)m};
+      const cuuint64_t tstr[1] = {(cuuint64_t)g.nlines * 4};
+      ok = encode_rows(&cp.tm_tmp, tmp, 2, tdims, tstr, (cuuint32_t)(COL_ROWS >> k));
+    }
+    if (!ok) {
+      if (tmp) scratch_free(tmp, stream);
+      return 0;
+    }
+    RegParams<T>& r = cp.r;
+    r.in = a.in;
+    r.out = a.out;
+    r.tmp = tmp;
+    r.tmp_line = 1;
+    r.tmp_pos = g.nlines;
+    r.g = g;
+    r.levels = a.levels;
+    r.nreg = k;
+    r.tpl = COL_CHUNKS;
+    r.lpc = COL_LANES;
+    r.tile = tile;
+    r.halo = halo;
+    r.ntiles = ntr;
+    r.prog = *a.prog;
+    cp.ncols = ncols;
+    cp.nouter = g.nother == 2 ? g.oshape[1] : 1;
+    cp.ntr = ntr;
+    cp.ntiles = ncols / COL_LANES * ntr * cp.nouter;
+    cp.rank3 = rank == 3;
+    cp.a_from_tmp = more ? 1 : 0;
+    cp.spin_limit = 1 << 22;
+    cp.err = err;
+    const int hmax = cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1;
+    const size_t smem = col_smem_bytes(hmax);
+    const int grid = (int)std::min<int64_t>(cp.ntiles, sm_count());
+
+    // band geometry: one other dim of nlines lines in tmp [position][line]
+    LineGeom gt;
+    std::memset(&gt, 0, sizeof(gt));
+    gt.n = m;
+    gt.nlines = g.nlines;
+    gt.nother = g.nother;
+    int64_t acc = 1;
+    for (int d = 0; d < g.nother; ++d) {
+      gt.oshape[d] = g.oshape[d];
+      gt.oin[d] = acc;
+      gt.oout[d] = acc;
+      acc *= g.oshape[d];
+    }
+    const bool fwd = (op == TF_F || op == TF_IA);
+    int rc = 1;
+    cudaError_t e = cudaSuccess;
+    if (!fwd && more) {
+      LineGeom g2 = gt;
+      g2.sin = g.sin;
+      g2.sout = g.nlines;
+      for (int d = 0; d < g.nother; ++d) g2.oin[d] = g.oin[d];
+      const int r2 = launch_whole<T>(a, g2, a.in, tmp, a.levels - k, true, stream, stats);
+      if (r2 != 1) rc = r2 == 0 ? -2 : r2;
+    }
+    if (rc == 1) {
+      e = fn(cp, grid, smem, stream);
+      if (e != cudaSuccess) rc = -(int)e - 1000;
+      else if (stats) stats->launches += 1;
+    }
+    if (rc == 1 && fwd && more) {
+      LineGeom g2 = gt;
+      g2.sin = g.nlines;
+      g2.sout = g.sout;
+      for (int d = 0; d < g.nother; ++d) g2.oout[d] = g.oout[d];
+      const int r2 = launch_whole<T>(a, g2, tmp, a.out, a.levels - k, true, stream, stats);
+      if (r2 != 1) rc = r2 == 0 ? -2 : r2;
+    }
+    if (tmp) scratch_free(tmp, stream);
+    return rc;
+  }
+}
+
 }  // namespace
+
+int check_col_errors(cudaStream_t stream) {
+  int32_t* f = col_error_flag();
+  if (!f) return 0;
+  int32_t v = 0;
+  if (cudaStreamSynchronize(stream) != cudaSuccess ||
+      cudaMemcpy(&v, f, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  if (v) cudaMemset(f, 0, sizeof(int32_t));
+  return v;
+}
 
 template <typename T>
 int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
@@ -328,7 +540,9 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
     if (rc != 0) return rc;
   }
   if (lines_adjacent(g)) {
-    int rc = launch_whole<T>(a, g, a.in, a.out, a.levels, true, stream, stats);
+    int rc = launch_col<T>(a, stream, stats);
+    if (rc != 0) return rc;
+    rc = launch_whole<T>(a, g, a.in, a.out, a.levels, true, stream, stats);
     if (rc != 0) return rc;
     return launch_tiled<T>(a, stream, stats);
   }

@@ -96,3 +96,30 @@ def test_other_boundaries_fall_back_exactly():
             rc, o = po.oracle_sep(x, 100907, tf, bc, [1, 0], [4, 3])
             g, _ = run(x, 100907, tf, bc, [1, 0], [4, 3])
             assert rc == 0 and np.array_equal(g, o), (bc, tf)
+
+
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_tma_strided_windows_and_whole_lines(op):
+    """Strided float32 passes on the TMA-staged kernel (line counts that are
+    multiples of 32): 2D columns with 512-sample windows and halos, whole
+    lines up to 512, a 3D view (rank-3 tensor maps), in place; bit for bit
+    against the oracle and against the kernels the option switches to."""
+    rng = np.random.default_rng(26 + op)
+    cases = [((4096, 64), [0], [6]), ((1024, 96), [0], [3]), ((2048, 32), [0], [1]),
+             ((512, 64), [0], [4]), ((256, 32), [0], [5]), ((64, 32, 128), [0, 1], [3, 2]),
+             ((96, 64), [1, 0], [2, 5])]
+    for w in WAVELETS:
+        for shape, axes, lv in cases:
+            x = rng.standard_normal(shape).astype(np.float32)
+            rc, o = po.oracle_sep(x, w, op, 0, axes, lv)
+            if rc:
+                continue
+            g, _ = run(x, w, op, 0, axes, lv)
+            assert np.array_equal(g, o), (w, shape, axes, lv)
+            _lib.set_option("tma_strided", 0)
+            try:
+                g2, _ = run(x, w, op, 0, axes, lv)
+            finally:
+                _lib.set_option("tma_strided", 1)
+            assert np.array_equal(g, g2)
+    assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
