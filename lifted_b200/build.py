@@ -93,7 +93,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     if force or tasks or not LIB.exists() or LIB.stat().st_mtime < newest:
         tmp = LIB.with_suffix(".so.tmp")
         _run([NVCC] + GENCODE + ["-shared", "-o", str(tmp)] +
-             [str(o) for o in objs] + ["-lcuda"])
+             [str(o) for o in objs])
         os.replace(tmp, LIB)
     return LIB
 
