@@ -282,7 +282,8 @@ LIFTED_CAPI uint64_t lifted_launch_count(void);
  *                               when a line fits in shared memory
  *   "max_global_ctas"      n    CTAs of the global-scratch line path
  *   "fast_path"            0/1  register-blocked kernels where they apply
- *   "tma_strided"          0/1  TMA-staged kernel for strided float32 passes */
+ *   "tma_strided"          0/1  TMA-staged kernel for strided float32 passes
+ *   "tma_packed"           0/1  two adjacent lines per lane in that kernel */
 LIFTED_CAPI int lifted_set_option(const char* name, int64_t value);
 /* Synchronises `stream` and reports LIFTED_ETIMEOUT if a kernel of this
  * library gave up a bounded device-side wait since the last check (the

@@ -1,22 +1,30 @@
 // Persistent TMA-staged kernel for strided axes (float32): the first k
-// levels of an axis pass on windows of 512 samples x 32 adjacent lines.
+// levels of an axis pass on windows of 512 samples x 32*V adjacent lines.
 //
 // The lines of a strided axis pass are columns of a 2D (or 3D) view whose
-// fastest dimension is contiguous: 32 adjacent lines give 128-byte rows.  A
-// CTA (512 threads: lane = line, 16 chunks of 32 samples along the axis)
-// loops over its tiles.  For each tile one thread issues TMA copies
-// (cp.async.bulk.tensor with 2D/3D boxes, completion on an mbarrier) of the
-// tile's rows into a 64 KiB staging buffer; every thread then moves its
-// chunk from the staging buffer into registers, the CTA releases the buffer
-// and the TMA engine fetches the next tile while the CTA lifts and stores
-// the current one.  Forward-stepping passes stage the raw window (two boxes
-// of 256 rows); reverse-stepping passes stage the window of every detail
-// band d_1 .. d_k and of the approximation band a_k (one box each).
+// fastest dimension is contiguous: 32*V adjacent lines give 128*V-byte rows.
+// A CTA (512 threads: lane = V adjacent lines, 16 chunks of 32 samples along
+// the axis) loops over its tiles.  For each tile one thread issues TMA
+// copies (cp.async.bulk.tensor with 2D/3D boxes, completion on an mbarrier)
+// of the tile's rows into the staging buffer; the threads move their chunks
+// into registers, the CTA releases the buffer and the TMA engine fetches the
+// next tile while the CTA lifts and stores the current one.
 //
+//   forward-stepping  stages the raw window (two boxes of 256 rows); every
+//                     thread takes its whole chunk, then the buffer is free;
+//   reverse-stepping  stages the window of every detail band d_1 .. d_k and
+//                     of the approximation band a_k (one box each); threads
+//                     take d_1 at once and read the coarser bands level by
+//                     level, and the buffer is released after the last of
+//                     those reads (level 2), so the next tile's copy overlaps
+//                     the two finest levels.
+//
+// With V = 2 a lane holds two adjacent lines and every step runs on packed
+// FP32x2 arithmetic (lw_reg_kernel.cuh, LaneVec), halving the instructions.
 // The lifting arithmetic, the mailbox neighbour exchange and the band
-// stores are those of the register-blocked kernel (lw_reg_kernel.cuh,
-// tile mode): interior results are exact, the halo absorbs the corrupted
-// window margins, out-of-band taps are skipped (Zero boundary).
+// stores are those of the register-blocked kernel in tile mode: interior
+// results are exact, the halo absorbs the corrupted window margins,
+// out-of-band taps are skipped (Zero boundary).
 #pragma once
 
 #include <cuda.h>
@@ -28,7 +36,7 @@
 namespace lw {
 
 constexpr int COL_P0 = 16;                             // pairs per chunk
-constexpr int COL_LANES = 32;                          // lines per tile
+constexpr int COL_LANES = 32;                          // lanes per row
 constexpr int COL_CHUNKS = 16;                         // chunks per window
 constexpr int COL_ROWS = 2 * COL_P0 * COL_CHUNKS;      // 512 window samples
 constexpr int COL_THREADS = COL_LANES * COL_CHUNKS;    // 512
@@ -36,15 +44,15 @@ constexpr int COL_MAXK = 5;                            // levels per tile launch
 
 struct ColParams {
   // tm_rows[i]: the input viewed as {lines (x), axis (y)[, outer (z)]},
-  // box {32, 256 >> i[, 1]}; tm_tmp: the approximation band buffer
-  // [position][line], box {32, 512 >> k}.
+  // box {32*V, 256 >> i[, 1]}; tm_tmp: the approximation band buffer
+  // [position][line], box {32*V, 512 >> k}.
   CUtensorMap tm_rows[COL_MAXK];
   CUtensorMap tm_tmp;
   RegParams<float> r;   // geometry, program, tile, band buffer, levels
-  int64_t ncols;        // lines along x (multiple of 32)
+  int64_t ncols;        // lines along x (multiple of 32*V)
   int64_t nouter;       // z extent (1 for a 2D view)
   int64_t ntr;          // row tiles per strip
-  int64_t ntiles;       // ncols/32 * ntr * nouter
+  int64_t ntiles;       // ncols/(32*V) * ntr * nouter
   int32_t rank3;        // tensor maps are 3D
   int32_t a_from_tmp;   // reverse: a_k is in the band buffer (else in `in`)
   int32_t spin_limit;   // mbarrier polls before giving up
@@ -106,84 +114,109 @@ struct TileCoord {
   int64_t outer, col0, rt, wstart;
 };
 
+template <int V>
 __device__ __forceinline__ TileCoord decode(const ColParams& p, int64_t t) {
-  const int64_t nstrips = p.ncols / COL_LANES;
+  const int64_t nstrips = p.ncols / (COL_LANES * V);
   const int64_t per_outer = nstrips * p.ntr;
   TileCoord c;
   c.outer = t / per_outer;
   const int64_t rem = t - c.outer * per_outer;
   const int64_t strip = rem / p.ntr;
   c.rt = rem - strip * p.ntr;
-  c.col0 = strip * COL_LANES;
+  c.col0 = strip * COL_LANES * V;
   c.wstart = c.rt * p.r.tile - p.r.halo;
   return c;
 }
 
 // Issues the TMA copies of tile t into the staging buffer (one thread).
-template <bool FWD>
+template <bool FWD, int V>
 __device__ __forceinline__ void issue(const ColParams& p, int64_t t, float* stage,
                                       uint64_t* bar) {
-  const TileCoord tc = decode(p, t);
+  constexpr int W = COL_LANES * V;  // floats per staging row
+  const TileCoord tc = decode<V>(p, t);
   const int x = (int)tc.col0, z = (int)tc.outer;
   const bool r3 = p.rank3 != 0;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_expect(bar, COL_ROWS * W * sizeof(float));
   if (FWD) {
-    mbar_expect(bar, COL_ROWS * COL_LANES * sizeof(float));
     tma_box(stage, &p.tm_rows[0], x, (int)tc.wstart, z, r3, bar);
-    tma_box(stage + 256 * COL_LANES, &p.tm_rows[0], x, (int)tc.wstart + 256, z, r3, bar);
+    tma_box(stage + 256 * W, &p.tm_rows[0], x, (int)tc.wstart + 256, z, r3, bar);
   } else {
     // d_l windows at rows m_l + (wstart >> l), l = 1..k, then a_k
     const int k = p.r.nreg;
-    mbar_expect(bar, COL_ROWS * COL_LANES * sizeof(float));
     int row = 0;
     for (int l = 1; l <= k; ++l) {
       const int64_t ml = p.r.g.n >> l;
-      tma_box(stage + (size_t)row * COL_LANES, &p.tm_rows[l - 1], x,
-              (int)(ml + (tc.wstart >> l)), z, r3, bar);
+      tma_box(stage + (size_t)row * W, &p.tm_rows[l - 1], x, (int)(ml + (tc.wstart >> l)), z,
+              r3, bar);
       row += COL_ROWS >> l;
     }
     if (p.a_from_tmp) {
       // band buffer: x = line index, y = position
       const int64_t L0 = tc.outer * p.ncols + tc.col0;
-      tma_box(stage + (size_t)row * COL_LANES, &p.tm_tmp, (int)L0, (int)(tc.wstart >> k), 0,
-              false, bar);
+      tma_box(stage + (size_t)row * W, &p.tm_tmp, (int)L0, (int)(tc.wstart >> k), 0, false, bar);
     } else {
-      tma_box(stage + (size_t)row * COL_LANES, &p.tm_rows[k - 1], x, (int)(tc.wstart >> k), z,
-              r3, bar);
+      tma_box(stage + (size_t)row * W, &p.tm_rows[k - 1], x, (int)(tc.wstart >> k), z, r3, bar);
     }
   }
 }
 
-// Reverse-stepping register levels with the detail values preloaded:
-// dd[off(LV) + i] holds pair i of this chunk's d at level LV, where
-// off(LV) = sum_{l < LV} (P0 >> l).
-template <int LV, int P0>
-constexpr int dd_off() {
-  int o = 0;
-  for (int l = 0; l < LV; ++l) o += P0 >> l;
-  return o;
+// Per-tile state of the reverse levels: where the staged bands are and how
+// to hand the buffer back.
+struct RevStage {
+  const float* stage;
+  uint64_t* bar;
+  const ColParams* p;
+  int64_t next;  // next tile of this CTA (>= ntiles: none)
+};
+
+// Staging row of pair 0 of this chunk in the band region of level LV
+// (detail bands d_1.., region sizes 256, 128, ...) or of a_k (LV = k - 1).
+__device__ __forceinline__ int region_row(int lv) { return COL_ROWS - (COL_ROWS >> lv); }
+
+template <typename VT, int V, int P, int PA>
+__device__ __forceinline__ void read_rows(VT (&v)[PA], const float* stage, int row0, int lane) {
+  constexpr int W = COL_LANES * V;
+  const float* q = stage + (size_t)row0 * W + lane * V;
+#pragma unroll
+  for (int i = 0; i < P; ++i) v[i] = *reinterpret_cast<const VT*>(q + (size_t)i * W);
 }
 
-template <int WI, int OP, int P0, int HMAX, int LV>
-__device__ __forceinline__ void rev_levels_pre(float (&s)[P0], float (&d)[P0],
-                                               const float (&dd)[2 * P0], reg::Ctx<float>& c) {
+template <int WI, int OP, int P0, int HMAX, int V, int LV>
+__device__ __forceinline__ void rev_levels(typename LaneVec<float, V>::type (&s)[P0],
+                                           typename LaneVec<float, V>::type (&d)[P0],
+                                           const typename LaneVec<float, V>::type (&d1)[P0],
+                                           reg::Ctx<float>& c, const RevStage& rs) {
+  using VT = typename LaneVec<float, V>::type;
   constexpr int P = P0 >> LV;
   if constexpr (LV >= 0) {
     if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
-      if (LV < c.p->nreg) {
+      const int k = c.p->nreg;
+      if (LV < k) {
         const RegParams<float>& p = *c.p;
         const int64_t nb = c.n >> (LV + 1);
         const int64_t gp0 = c.e0 >> (LV + 1);
+        if constexpr (LV > 0) {
+          if (LV + 1 == k) read_rows<VT, V, P, P0>(s, rs.stage, region_row(k) + c.r * P, c.j);
+          read_rows<VT, V, P, P0>(d, rs.stage, region_row(LV) + c.r * P, c.j);
+          if (LV == 1) {
+            // last read of the staging buffer for this tile
+            __syncthreads();
+            if (c.tid == 0 && rs.next < rs.p->ntiles)
+              issue<false, V>(*rs.p, rs.next, const_cast<float*>(rs.stage), rs.bar);
+          }
+        } else {
 #pragma unroll
-        for (int i = 0; i < P; ++i) d[i] = dd[dd_off<LV, P0>() + i];
-        reg::steps<float, float, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
+          for (int i = 0; i < P0; ++i) d[i] = d1[i];
+        }
+        reg::steps<float, VT, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
         if constexpr (LV == 0) {
           if (reg::chunk_stored(c)) {
             float* o = p.out + c.bout + c.e0 * p.g.sout;
 #pragma unroll
             for (int i = 0; i < P; ++i) {
-              o[(2 * i) * p.g.sout] = s[i];
-              o[(2 * i + 1) * p.g.sout] = d[i];
+              *reinterpret_cast<VT*>(o + (2 * i) * p.g.sout) = s[i];
+              *reinterpret_cast<VT*>(o + (2 * i + 1) * p.g.sout) = d[i];
             }
           }
         } else {
@@ -194,25 +227,27 @@ __device__ __forceinline__ void rev_levels_pre(float (&s)[P0], float (&d)[P0],
           }
         }
       }
-      if constexpr (LV > 0) rev_levels_pre<WI, OP, P0, HMAX, LV - 1>(s, d, dd, c);
+      if constexpr (LV > 0) rev_levels<WI, OP, P0, HMAX, V, LV - 1>(s, d, d1, c, rs);
     } else if constexpr (LV > 0) {
-      rev_levels_pre<WI, OP, P0, HMAX, LV - 1>(s, d, dd, c);
+      rev_levels<WI, OP, P0, HMAX, V, LV - 1>(s, d, d1, c, rs);
     }
   }
 }
 
 }  // namespace col
 
-template <int WI, int OP>
+template <int WI, int OP, int V>
 __global__ void __launch_bounds__(COL_THREADS, 1)
     col_kernel(const __grid_constant__ ColParams p) {
+  using VT = typename LaneVec<float, V>::type;
   constexpr int P0 = COL_P0;
+  constexpr int W = COL_LANES * V;
   constexpr int HMAX = cat_reach(WI, OP) > 0 ? cat_reach(WI, OP) : 1;
   constexpr bool FWD = (OP == TF_F || OP == TF_IA);
   extern __shared__ __align__(128) unsigned char col_smem[];
   float* stage = reinterpret_cast<float*>(col_smem);
-  float* mbox = stage + COL_ROWS * COL_LANES;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(mbox + 4 * HMAX * COL_THREADS);
+  float* mbox = stage + COL_ROWS * W;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(mbox + 4 * HMAX * COL_THREADS * V);
 
   const int tid = threadIdx.x;
   reg::Ctx<float> c;
@@ -234,7 +269,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   __syncthreads();
   uint32_t parity = 0;
   int64_t t = blockIdx.x;
-  if (t < p.ntiles && tid == 0) col::issue<FWD>(p, t, stage, bar);
+  if (t < p.ntiles && tid == 0) col::issue<FWD, V>(p, t, stage, bar);
   for (; t < p.ntiles; t += gridDim.x) {
     const bool got = col::mbar_wait(bar, parity, p.spin_limit);
     if (!__syncthreads_and(got)) {
@@ -243,10 +278,10 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
       return;
     }
     parity ^= 1;
-    const col::TileCoord tc = col::decode(p, t);
-    const int64_t L = tc.outer * p.ncols + tc.col0 + c.j;
+    const col::TileCoord tc = col::decode<V>(p, t);
+    const int64_t L = tc.outer * p.ncols + tc.col0 + (int64_t)c.j * V;
     c.L = L;
-    c.line_ok = L < p.r.g.nlines;
+    c.line_ok = L < p.r.g.nlines;  // V lines together (ncols % (32 V) == 0)
     c.bin = 0;
     c.bout = 0;
     if (c.line_ok) line_base(p.r.g, L, c.bin, c.bout);
@@ -254,44 +289,31 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
     c.e0 = tc.wstart + (int64_t)2 * P0 * c.r;
     c.tile_lo = tc.rt * p.r.tile;
     c.tile_hi = c.tile_lo + p.r.tile < c.n ? c.tile_lo + p.r.tile : c.n;
+    const int64_t next = t + gridDim.x;
 
-    float s[P0], d[P0];
-    float dd[2 * P0];
+    VT s[P0], d[P0];
     if constexpr (FWD) {
-      const float* st = stage + (size_t)(c.r * 2 * P0) * COL_LANES + c.j;
+      const float* st = stage + (size_t)(c.r * 2 * P0) * W + c.j * V;
 #pragma unroll
       for (int i = 0; i < P0; ++i) {
-        s[i] = st[(2 * i) * COL_LANES];
-        d[i] = st[(2 * i + 1) * COL_LANES];
+        s[i] = *reinterpret_cast<const VT*>(st + (size_t)(2 * i) * W);
+        d[i] = *reinterpret_cast<const VT*>(st + (size_t)(2 * i + 1) * W);
       }
+      __syncthreads();  // staging consumed
+      if (tid == 0 && next < p.ntiles) col::issue<FWD, V>(p, next, stage, bar);
+      reg::fwd_levels<float, VT, V, WI, OP, P0, HMAX, 0, true>(s, d, c);
     } else {
       const int k = p.r.nreg;
-      int row = 0;
-#pragma unroll
-      for (int lv = 0; lv < COL_MAXK; ++lv) {
-        if (lv < k) {
-          const int P = P0 >> lv;
-          const float* st = stage + (size_t)(row + c.r * P) * COL_LANES + c.j;
-          const int off = (2 * P0) - (2 * P0 >> lv);  // sum_{l<lv} P0 >> l
-#pragma unroll
-          for (int i = 0; i < (P0 >> lv); ++i) dd[off + i] = st[i * COL_LANES];
-          row += COL_ROWS >> (lv + 1);
-        }
+      VT d1[P0];
+      col::read_rows<VT, V, P0, P0>(d1, stage, c.r * P0, c.j);  // d_1 region
+      if (k == 1) {
+        col::read_rows<VT, V, P0, P0>(s, stage, col::region_row(1) + c.r * P0, c.j);
+        __syncthreads();
+        if (tid == 0 && next < p.ntiles) col::issue<FWD, V>(p, next, stage, bar);
       }
-      const int Pa = P0 >> (k - 1);
-      const float* st = stage + (size_t)(row + c.r * Pa) * COL_LANES + c.j;
-#pragma unroll
-      for (int i = 0; i < P0; ++i)
-        if (i < Pa) s[i] = st[i * COL_LANES];
-    }
-    __syncthreads();  // staging consumed
-    if (tid == 0 && t + gridDim.x < p.ntiles) col::issue<FWD>(p, t + gridDim.x, stage, bar);
-
-    if constexpr (FWD) {
-      reg::fwd_levels<float, float, 1, WI, OP, P0, HMAX, 0, true>(s, d, c);
-    } else {
+      col::RevStage rs{stage, bar, &p, next};
       constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
-      col::rev_levels_pre<WI, OP, P0, HMAX, TOP>(s, d, dd, c);
+      col::rev_levels<WI, OP, P0, HMAX, V, TOP>(s, d, d1, c, rs);
     }
   }
 }

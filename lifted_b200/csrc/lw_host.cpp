@@ -70,6 +70,7 @@ std::atomic<int64_t> g_opt_force_global{0};
 std::atomic<int64_t> g_opt_max_global_ctas{296};
 std::atomic<int64_t> g_opt_fast_path{1};
 std::atomic<int64_t> g_opt_tma_strided{1};
+std::atomic<int64_t> g_opt_tma_packed{1};
 
 }  // namespace
 
@@ -796,6 +797,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_fast_path = value ? 1 : 0;
   } else if (!std::strcmp(name, "tma_strided")) {
     g_opt_tma_strided = value ? 1 : 0;
+  } else if (!std::strcmp(name, "tma_packed")) {
+    g_opt_tma_packed = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");
@@ -807,6 +810,7 @@ int set_option(const char* name, int64_t value) {
 }
 uint64_t launch_count() { return g_launches.load(); }
 bool col_enabled() { return g_opt_tma_strided.load() != 0; }
+bool col_packed() { return g_opt_tma_packed.load() != 0; }
 
 }  // namespace lw
 

@@ -33,6 +33,8 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats)
 // Whether strided float32 passes may use the TMA-staged kernel (the
 // "tma_strided" option; on by default).
 bool col_enabled();
+// Whether it may pack two adjacent lines per lane (the "tma_packed" option).
+bool col_packed();
 // Synchronises `stream`; returns 1 (and clears it) if a TMA-staged kernel
 // gave up waiting for a staging copy since the last check, 0 if not, -1 if
 // the check itself failed.

@@ -376,10 +376,10 @@ EncodeTiledFn encode_tiled_fn() {
 }
 
 bool encode_rows(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims,
-                 const cuuint64_t* strides, cuuint32_t box_y) {
+                 const cuuint64_t* strides, cuuint32_t box_x, cuuint32_t box_y) {
   EncodeTiledFn enc = encode_tiled_fn();
   if (!enc) return false;
-  const cuuint32_t box[3] = {(cuuint32_t)COL_LANES, box_y, 1};
+  const cuuint32_t box[3] = {box_x, box_y, 1};
   const cuuint32_t es[3] = {1, 1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<void*>(base),
              dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -406,7 +406,13 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     const int64_t n = g.n;
     if (n % 32) return 0;
     const int wi = a.wi, op = a.op;
-    ColFn fn = pick_col(wi, op);
+    // two adjacent lines per lane (packed FP32x2) when the line groups and
+    // every line base of the output stay 8-byte aligned
+    int v = 1;
+    if (col_packed() && ncols % (2 * COL_LANES) == 0 && (g.sout % 2) == 0 &&
+        (g.nother < 2 || (g.oout[1] % 2) == 0) && (reinterpret_cast<uintptr_t>(a.out) & 7) == 0)
+      v = 2;
+    ColFn fn = pick_col(wi, op, v);
     if (!fn) return 0;
     const int maxreg = std::min(reg_max_levels(wi, op, COL_P0), COL_MAXK);
     int k = 0;
@@ -452,12 +458,13 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     const cuuint64_t strides[2] = {(cuuint64_t)g.sin * 4,
                                    (cuuint64_t)(g.nother == 2 ? g.oin[1] : 0) * 4};
     bool ok = true;
+    const cuuint32_t bx = (cuuint32_t)(COL_LANES * v);
     for (int i = 0; i < k && ok; ++i)
-      ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, (cuuint32_t)(256 >> i));
+      ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, bx, (cuuint32_t)(256 >> i));
     if (ok && more) {
       const cuuint64_t tdims[2] = {(cuuint64_t)g.nlines, (cuuint64_t)m};
       const cuuint64_t tstr[1] = {(cuuint64_t)g.nlines * 4};
-      ok = encode_rows(&cp.tm_tmp, tmp, 2, tdims, tstr, (cuuint32_t)(COL_ROWS >> k));
+      ok = encode_rows(&cp.tm_tmp, tmp, 2, tdims, tstr, bx, (cuuint32_t)(COL_ROWS >> k));
     }
     if (!ok) {
       if (tmp) scratch_free(tmp, stream);
@@ -481,13 +488,13 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     cp.ncols = ncols;
     cp.nouter = g.nother == 2 ? g.oshape[1] : 1;
     cp.ntr = ntr;
-    cp.ntiles = ncols / COL_LANES * ntr * cp.nouter;
+    cp.ntiles = ncols / (COL_LANES * v) * ntr * cp.nouter;
     cp.rank3 = rank == 3;
     cp.a_from_tmp = more ? 1 : 0;
     cp.spin_limit = 1 << 22;
     cp.err = err;
     const int hmax = cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1;
-    const size_t smem = col_smem_bytes(hmax);
+    const size_t smem = col_smem_bytes(hmax, v);
     const int grid = (int)std::min<int64_t>(cp.ntiles, sm_count());
 
     // band geometry: one other dim of nlines lines in tmp [position][line]
