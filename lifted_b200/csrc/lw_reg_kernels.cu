@@ -386,6 +386,10 @@ bool encode_rows(CUtensorMap* m, const void* base, int rank, const cuuint64_t* d
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+template <typename T>
+int band_pass(const RegPassArgs<T>& a, const LineGeom& g2, const T* in, T* out, int levels,
+              cudaStream_t stream, RegStats* stats);
+
 // Strided float32 pass on the TMA-staged persistent kernel: whole lines of
 // up to 512 samples, or 512-sample windows with halos on longer lines; the
 // levels beyond the first k run as a strided whole-line launch on the
@@ -412,8 +416,6 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (col_packed() && ncols % (2 * COL_LANES) == 0 && (g.sout % 2) == 0 &&
         (g.nother < 2 || (g.oout[1] % 2) == 0) && (reinterpret_cast<uintptr_t>(a.out) & 7) == 0)
       v = 2;
-    ColFn fn = pick_col(wi, op, v);
-    if (!fn) return 0;
     const int maxreg = std::min(reg_max_levels(wi, op, COL_P0), COL_MAXK);
     int k = 0;
     int64_t tile, halo, ntr;
@@ -438,6 +440,11 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       ntr = (n + tile - 1) / tile;
     }
     if (k < 1) return 0;
+    // packed lanes only while they still give every SM a tile
+    if (v == 2 && ncols / (2 * COL_LANES) * ntr * (g.nother == 2 ? g.oshape[1] : 1) < sm_count())
+      v = 1;
+    ColFn fn = pick_col(wi, op, v);
+    if (!fn) return 0;
     const int64_t m = n >> k;
     const bool more = a.levels > k;
     if (more && ((m % 32) || m / 32 > 16)) return 0;
@@ -518,7 +525,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       g2.sin = g.sin;
       g2.sout = g.nlines;
       for (int d = 0; d < g.nother; ++d) g2.oin[d] = g.oin[d];
-      const int r2 = launch_whole<T>(a, g2, a.in, tmp, a.levels - k, true, stream, stats);
+      const int r2 = band_pass<T>(a, g2, a.in, tmp, a.levels - k, stream, stats);
       if (r2 != 1) rc = r2 == 0 ? -2 : r2;
     }
     if (rc == 1) {
@@ -531,12 +538,31 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       g2.sin = g.nlines;
       g2.sout = g.sout;
       for (int d = 0; d < g.nother; ++d) g2.oout[d] = g.oout[d];
-      const int r2 = launch_whole<T>(a, g2, tmp, a.out, a.levels - k, true, stream, stats);
+      const int r2 = band_pass<T>(a, g2, tmp, a.out, a.levels - k, stream, stats);
       if (r2 != 1) rc = r2 == 0 ? -2 : r2;
     }
     if (tmp) scratch_free(tmp, stream);
     return rc;
   }
+}
+
+// The levels past a tile launch, on the approximation band (lines adjacent
+// in memory on at least one side): the TMA-staged kernel when the band
+// qualifies (whole lines of up to 512), else the register kernel.
+template <typename T>
+int band_pass(const RegPassArgs<T>& a, const LineGeom& g2, const T* in, T* out, int levels,
+              cudaStream_t stream, RegStats* stats) {
+  if (g2.oin[0] == 1 && g2.oout[0] == 1) {
+    RegPassArgs<T> b = a;
+    b.g = g2;
+    b.in = in;
+    b.out = out;
+    b.levels = levels;
+    b.in_place = false;
+    const int rc = launch_col<T>(b, stream, stats);
+    if (rc != 0) return rc;
+  }
+  return launch_whole<T>(a, g2, in, out, levels, true, stream, stats);
 }
 
 }  // namespace
