@@ -289,6 +289,50 @@ def batched_section(dev, plain_sample: int = 300, steps: int = 5):
             "speedup_vs_plain": round(gbs / plain_gbs, 1)}
 
 
+def cfg1_section(dev, steps: int = 10):
+    """Plain 1D float64: 64 signals of 65536 i.i.d. N(0,1) (seed 1001),
+    Daubechies2, 5 levels along axis 1, Zero boundary, Forward then
+    ForwardAdjoint (the long lines run on the batch engine, many CTAs per
+    line), timed as a CUDA graph replay; plus the dot-product test
+    <W x, r> = <x, W^T r>."""
+    import torch
+    from lifted_b200 import pylifted as pl
+
+    g = torch.Generator(device=dev).manual_seed(1001)
+    x = torch.randn(64, 65536, dtype=torch.float64, device=dev, generator=g)
+    r = torch.randn(64, 65536, dtype=torch.float64, device=dev, generator=g)
+    w = torch.empty_like(x)
+    y = torch.empty_like(x)
+
+    def step():
+        pl._lwt(x, 2, 0, 0, (1,), (5,), 1, out=w)
+        pl._lwt(w, 2, 0, 2, (1,), (5,), 1, out=y)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize(dev)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+        step()
+    graph.replay()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    wx = pl.lwt_forward(x, "db2", "Zero", axes=(1,), level=(5,))
+    wtr = pl.lwt_forward_adjoint(r, "db2", "Zero", axes=(1,), level=(5,))
+    a, b = float((wx * r).sum()), float((x * wtr).sum())
+    B = 2 * 2 * x.numel() * 8
+    return {"workload": "float64 64 x 65536 N(0,1) (seed 1001), Daubechies2, 5 levels on "
+                        "axis 1, Zero boundary, Forward + ForwardAdjoint",
+            "value": round(B / ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(ms, 4),
+            "dot_product_rel_err": abs(a - b) / abs(a)}
+
+
 def autograd_section(dev, steps: int = 10):
     """3D float32 512^3 (N(0,1) smoothed by an edge-clamped 3-point box per
     axis), Daubechies4, levels (4,4,4) on axes (0,1,2), through the
@@ -563,8 +607,9 @@ def main() -> int:
                              f"(reference sources + Highway stand-in, {variant}, "
                              f"{cores} threads)"}
 
-    extras = {"batched": None, "autograd": None, "lsq": None}
+    extras = {"cfg1_1d_f64": None, "batched": None, "autograd": None, "lsq": None}
     if world == 1 and not args.no_extras:
+        extras["cfg1_1d_f64"] = cfg1_section(dev)
         extras["batched"] = batched_section(dev)
         extras["autograd"] = autograd_section(dev)
         extras["lsq"] = lsq_section(dev)
@@ -596,6 +641,7 @@ def main() -> int:
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "cfg1_1d_f64": extras["cfg1_1d_f64"],
             "batched": extras["batched"],
             "autograd": extras["autograd"],
             "lsq": extras["lsq"],

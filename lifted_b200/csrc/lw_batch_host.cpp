@@ -39,6 +39,8 @@ struct lifted_batch_plan {
   int32_t spin_limit = 4000000;
   int64_t ntile = 0, nwhole = 0, nwhole_global = 0, nsignals = 0;
   int64_t max_in = 0, max_out = 0;  // highest element index + 1 touched
+  // completion of the last run, so that a run on another stream starts after it
+  cudaEvent_t last = nullptr;
   // captured graph of one run and the pointers it was captured with
   cudaGraphExec_t gexec = nullptr;
   const void* g_in = nullptr;
@@ -505,6 +507,10 @@ int ensure_device(lifted_batch_plan* p) {
     return set_error(e == cudaErrorMemoryAllocation ? LIFTED_ENOMEM : LIFTED_ECUDA,
                      "batch plan buffers: %s", cudaGetErrorString(e));
   }
+  if (cudaEventCreateWithFlags(&p->last, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    p->last = nullptr;
+  }
   p->device = dev;
   return LIFTED_OK;
 }
@@ -524,6 +530,11 @@ int plan_run(lifted_batch_plan* p, const T* in, T* out, cudaStream_t stream,
     return set_error(LIFTED_EINVAL, "batch input and output overlap");
   int rc = ensure_device<T>(p);
   if (rc) return rc;
+  // runs of one plan share its queue and counters: order them on the GPU
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) cudaGetLastError();
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
+  if (p->last && !capturing) cudaStreamWaitEvent(stream, p->last, 0);
   cudaError_t e = cudaMemsetAsync(p->d_sync, 0, (size_t)(2 + p->ncounters) * sizeof(int32_t), stream);
   if (e != cudaSuccess) return set_error(LIFTED_ECUDA, "batch reset: %s", cudaGetErrorString(e));
   BatchParams<T> bp;
@@ -543,6 +554,7 @@ int plan_run(lifted_batch_plan* p, const T* in, T* out, cudaStream_t stream,
   e = launch_batch(bp, p->grid, p->block, p->smem, stream);
   if (count) count_launches(1);
   if (e != cudaSuccess) return set_error(LIFTED_ECUDA, "batch kernel launch: %s", cudaGetErrorString(e));
+  if (p->last && !capturing) cudaEventRecord(p->last, stream);
   return LIFTED_OK;
 }
 
@@ -594,6 +606,92 @@ int plan_graph(lifted_batch_plan* p, const void* in, void* out, cudaStream_t str
   if (e != cudaSuccess) return set_error(LIFTED_ECUDA, "graph launch: %s", cudaGetErrorString(e));
   return LIFTED_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Long contiguous lines of an axis pass as a batch (each line one signal).
+
+struct LinesKey {
+  std::string k;
+  bool operator<(const LinesKey& o) const { return k < o.k; }
+};
+std::mutex g_lines_mu;
+std::map<LinesKey, lifted_batch_plan*> g_lines_plans;
+std::vector<LinesKey> g_lines_order;  // insertion order, oldest first
+constexpr size_t kLinesPlans = 16;
+
+}  // namespace
+
+template <typename T>
+int run_lines_batched(uint32_t wavelet, int op, int bc, const LineGeom& g, int levels,
+                      const T* in, T* out, cudaStream_t stream) {
+  if (g.sin != 1 || g.sout != 1 || levels < 1 || g.nlines < 1) return 0;
+  for (int d = 0; d < g.nother; ++d)
+    if (g.oin[d] < 0 || g.oout[d] < 0) return 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  char buf[96];
+  std::string key;
+  std::snprintf(buf, sizeof(buf), "%d|%d|%u|%d|%d|%d|%lld|%lld|", dev, (int)sizeof(T), wavelet,
+                op, bc, levels, (long long)g.n, (long long)g.nlines);
+  key = buf;
+  for (int d = 0; d < g.nother; ++d) {
+    std::snprintf(buf, sizeof(buf), "%lld,%lld,%lld;", (long long)g.oshape[d],
+                  (long long)g.oin[d], (long long)g.oout[d]);
+    key += buf;
+  }
+  std::lock_guard<std::mutex> lk(g_lines_mu);
+  lifted_batch_plan* plan = nullptr;
+  auto it = g_lines_plans.find({key});
+  if (it != g_lines_plans.end()) {
+    plan = it->second;
+  } else {
+    std::vector<lifted_signal_t> sig((size_t)g.nlines);
+    for (int64_t L = 0; L < g.nlines; ++L) {
+      int64_t r = L, bi = 0, bo = 0;
+      for (int d = 0; d < g.nother; ++d) {
+        const int64_t q = r / g.oshape[d];
+        const int64_t idx = r - q * g.oshape[d];
+        r = q;
+        bi += idx * g.oin[d];
+        bo += idx * g.oout[d];
+      }
+      sig[L].wavelet = wavelet;
+      sig[L].levels = (uint32_t)levels;
+      sig[L].length = (uint64_t)g.n;
+      sig[L].in_offset = (uint64_t)bi;
+      sig[L].out_offset = (uint64_t)bo;
+    }
+    const int rc = plan_create<T>((uint32_t)op, (uint32_t)bc, sig.size(), sig.data(), nullptr, &plan);
+    if (rc) {
+      clear_error();
+      return 0;  // not eligible: the general path handles it
+    }
+    if (g_lines_plans.size() >= kLinesPlans) {
+      const LinesKey old = g_lines_order.front();
+      g_lines_order.erase(g_lines_order.begin());
+      lifted_batch_plan* victim = g_lines_plans[old];
+      g_lines_plans.erase(old);
+      // a run still in flight keeps using the buffers: wait for it first
+      if (victim->last) cudaEventSynchronize(victim->last);
+      lifted_batch_plan_destroy(victim);
+    }
+    g_lines_plans[{key}] = plan;
+    g_lines_order.push_back({key});
+  }
+  const int rc = plan_run<T>(plan, in, out, stream);
+  if (rc) return -1;
+  return 1;
+}
+
+template int run_lines_batched<float>(uint32_t, int, int, const LineGeom&, int, const float*,
+                                      float*, cudaStream_t);
+template int run_lines_batched<double>(uint32_t, int, int, const LineGeom&, int,
+                                       const double*, double*, cudaStream_t);
+
+namespace {
 
 // ---------------------------------------------------------------------------
 // Autotuner.
@@ -766,6 +864,7 @@ LIFTED_CAPI int lifted_batch_plan_item(const lifted_batch_plan_t* plan, size_t i
 LIFTED_CAPI void lifted_batch_plan_destroy(lifted_batch_plan_t* plan) {
   if (!plan) return;
   if (plan->gexec) cudaGraphExecDestroy(plan->gexec);
+  if (plan->last) cudaEventDestroy(plan->last);
   if (plan->d_items) cudaFree(plan->d_items);
   if (plan->d_progs) cudaFree(plan->d_progs);
   if (plan->d_sync) cudaFree(plan->d_sync);

@@ -71,6 +71,7 @@ std::atomic<int64_t> g_opt_max_global_ctas{296};
 std::atomic<int64_t> g_opt_fast_path{1};
 std::atomic<int64_t> g_opt_tma_strided{1};
 std::atomic<int64_t> g_opt_tma_packed{1};
+std::atomic<int64_t> g_opt_long_batched{1};
 
 }  // namespace
 
@@ -415,6 +416,26 @@ int run_axis_pass(const Program& prog, int op, int bc, int across,
   const int64_t pitch = n;
   const int64_t pitch_b = n - n / 2;
   const size_t line_bytes = (size_t)(pitch + pitch_b) * sizeof(T);
+  // Lines too long for one CTA's shared memory: many CTAs per line through
+  // the batch engine (level-group tiles), when the lines are contiguous and
+  // source and destination do not overlap.
+  if (line_bytes > kMaxDynSmem && prog.cat_index >= 0 && bc == BC_ZERO && !opt.force_global &&
+      !opt.no_alloc && opt.fast_path && g_opt_long_batched.load()) {
+    int64_t ilo = 0, ihi = 0, olo = 0, ohi = 0;
+    for (size_t d = 0; d < ndim; ++d) {
+      const int64_t ei = (shape[d] - 1) * sin[d], eo = (shape[d] - 1) * sout[d];
+      (ei < 0 ? ilo : ihi) += ei;
+      (eo < 0 ? olo : ohi) += eo;
+    }
+    const bool overlap = (const char*)(in + ilo) < (const char*)(out + ohi + 1) &&
+                         (const char*)(out + olo) < (const char*)(in + ihi + 1);
+    if (!overlap) {
+      const int rc = run_lines_batched<T>(wavelet_value((size_t)prog.cat_index), op, bc, g,
+                                          (int)levels, in, out, stream);
+      if (rc == 1) return LIFTED_OK;
+      if (rc < 0) return LIFTED_ECUDA;
+    }
+  }
   const bool contiguous_axis = (std::llabs(g.sin) == 1);
   int block = 256;
   int W = 1;
@@ -799,6 +820,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_tma_strided = value ? 1 : 0;
   } else if (!std::strcmp(name, "tma_packed")) {
     g_opt_tma_packed = value ? 1 : 0;
+  } else if (!std::strcmp(name, "long_lines_batched")) {
+    g_opt_long_batched = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");

@@ -1,6 +1,8 @@
 // Host-side interfaces of the B200 lifting DWT library.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
 #include <vector>
@@ -58,6 +60,13 @@ bool line_degenerate(const Program& prog, int op, int bc, int64_t n,
 size_t wavelet_count();
 uint32_t wavelet_value(size_t i);
 size_t wavelet_width(uint32_t w);
+
+// Runs the lines of an axis pass (contiguous, non-negative offsets) as a
+// cached batch plan of the batch engine, one signal per line: 1 done, 0 not
+// eligible, -1 failed (the error is set).
+template <typename T>
+int run_lines_batched(uint32_t wavelet, int op, int bc, const LineGeom& g, int levels,
+                      const T* in, T* out, cudaStream_t stream);
 
 template <typename T>
 int lwt_entry(const Program& prog, bool separable, uint32_t op, uint32_t bc,

@@ -193,3 +193,30 @@ def test_host_and_device_paths_agree():
     d = pl.lwt_forward(torch.from_numpy(x).cuda(), "cdf9.7", "Symmetric",
                        axes=(0, 1), level=(3, 4)).cpu().numpy()
     assert np.array_equal(h, d)
+
+
+@pytest.mark.parametrize("tf", [0, 1, 2, 3])
+def test_long_contiguous_lines_on_batch_engine(tf):
+    """Contiguous lines too long for one CTA (Zero boundary) run on the batch
+    engine, many CTAs per line; bit for bit against the oracle and against
+    the single-CTA general kernel (option off); a second call reuses the
+    cached plan."""
+    rng = np.random.default_rng(40 + tf)
+    for dt, shape, w, lv in ((np.float64, (4, 65536), 2, 5), (np.float32, (3, 100000), 10, 6),
+                             (np.float64, (2, 3, 40000), 203, 4)):
+        x = rng.standard_normal(shape).astype(dt)
+        ax = len(shape) - 1
+        rc, o = po.oracle_sep(x, w, tf, 0, [ax], [lv])
+        assert rc == 0
+        t = torch.from_numpy(x).cuda()
+        for _ in range(2):
+            n0 = _lib.launch_count()
+            g = pl._lwt(t, w, 0, tf, (ax,), (lv,), 1).cpu().numpy()
+            assert _lib.launch_count() - n0 == 1
+            assert np.array_equal(g, o), (dt, shape, w)
+        _lib.set_option("long_lines_batched", 0)
+        try:
+            g2 = pl._lwt(t, w, 0, tf, (ax,), (lv,), 1).cpu().numpy()
+        finally:
+            _lib.set_option("long_lines_batched", 1)
+        assert np.array_equal(g2, o)
