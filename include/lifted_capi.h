@@ -285,7 +285,9 @@ LIFTED_CAPI uint64_t lifted_launch_count(void);
  *   "tma_strided"          0/1  TMA-staged kernel for strided float32 passes
  *   "tma_packed"           0/1  two adjacent lines per lane in that kernel
  *   "long_lines_batched"   0/1  contiguous lines too long for one CTA run
- *                               on the batch engine (many CTAs per line) */
+ *                               on the batch engine (many CTAs per line)
+ *   "wrow_split"           0/1  float32 rows of 2048/4096 split over two
+ *                               warps (else one warp per row) */
 LIFTED_CAPI int lifted_set_option(const char* name, int64_t value);
 /* Synchronises `stream` and reports LIFTED_ETIMEOUT if a kernel of this
  * library gave up a bounded device-side wait since the last check (the

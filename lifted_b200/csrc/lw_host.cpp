@@ -72,6 +72,7 @@ std::atomic<int64_t> g_opt_fast_path{1};
 std::atomic<int64_t> g_opt_tma_strided{1};
 std::atomic<int64_t> g_opt_tma_packed{1};
 std::atomic<int64_t> g_opt_long_batched{1};
+std::atomic<int64_t> g_opt_wrow_split{1};
 
 }  // namespace
 
@@ -822,6 +823,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_tma_packed = value ? 1 : 0;
   } else if (!std::strcmp(name, "long_lines_batched")) {
     g_opt_long_batched = value ? 1 : 0;
+  } else if (!std::strcmp(name, "wrow_split")) {
+    g_opt_wrow_split = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");
@@ -834,6 +837,7 @@ int set_option(const char* name, int64_t value) {
 uint64_t launch_count() { return g_launches.load(); }
 bool col_enabled() { return g_opt_tma_strided.load() != 0; }
 bool col_packed() { return g_opt_tma_packed.load() != 0; }
+bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
 
 }  // namespace lw
 

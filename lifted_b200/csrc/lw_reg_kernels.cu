@@ -177,11 +177,34 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   return 1;
 }
 
-// Contiguous rows of 64 * P0 elements, every level in one warp's registers.
+// Contiguous rows of 64 * P0 elements, every level in one warp's registers
+// (or, for float32 rows of 2048 and 4096, in a pair of warps' registers).
 template <typename T>
 int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   const LineGeom& g = a.g;
   if (!rows_vectorisable(g, a.in, a.out)) return 0;
+  if constexpr (sizeof(T) == 4) {
+    const int64_t q0 = g.n / 128;
+    if (wrow2_enabled() && g.n % 128 == 0 && (q0 == 16 || q0 == 32) &&
+        wrow2_levels_f32(a.wi, a.op, (int)q0) >= a.levels) {
+      WRowParams<T> p;
+      std::memset(&p, 0, sizeof(p));
+      p.in = a.in;
+      p.out = a.out;
+      p.g = g;
+      p.levels = a.levels;
+      p.prog = *a.prog;
+      const size_t smem = (size_t)4 * (size_t)g.n * sizeof(T);
+      const int64_t grid = std::min<int64_t>((g.nlines + 1) / 2,
+                                             (int64_t)sm_count() * wrow2_resident_ctas((int)q0));
+      if (grid <= 0x7fffffffLL) {
+        cudaError_t e = launch_wrow2_f32(a.wi, a.op, (int)q0, p, (int)grid, smem, stream);
+        if (e != cudaSuccess) return -(int)e - 1000;
+        if (stats) stats->launches += 1;
+        return 1;
+      }
+    }
+  }
   if (g.n % 64) return 0;
   const int64_t p0 = g.n / 64;
   const int maxp0 = sizeof(T) == 4 ? 64 : 32;

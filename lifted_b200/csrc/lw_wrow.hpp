@@ -20,4 +20,15 @@ cudaError_t launch_wrow_f32(int wi, int op, int p0, const WRowParams<float>& p,
 cudaError_t launch_wrow_f64(int wi, int op, int p0, const WRowParams<double>& p,
                             int grid, int block, size_t smem, cudaStream_t stream);
 
+// Two warps per row (float32 rows of 128 * p0 elements, p0 16 or 32; 128
+// threads = two rows per CTA): levels compiled, 0 if none; launcher.
+int wrow2_levels_f32(int wi, int op, int p0);
+cudaError_t launch_wrow2_f32(int wi, int op, int p0, const WRowParams<float>& p, int grid,
+                             size_t smem, cudaStream_t stream);
+// CTAs per SM the two-warp kernel's shared memory allows (grid sizing of
+// the persistent launch).
+int wrow2_resident_ctas(int p0);
+// Whether contiguous float32 rows may use it (the "wrow_split" option).
+bool wrow2_enabled();
+
 }  // namespace lw

@@ -1,0 +1,74 @@
+// Instantiations of the two-warp-per-row kernel (lw_wrow2_kernel.cuh).
+#include <cuda_runtime.h>
+
+#include "lw_launch.hpp"
+#include "lw_wrow.hpp"
+#include "lw_wrow2_kernel.cuh"
+
+namespace lw {
+
+namespace {
+
+template <int WI, int OP, int P0>
+cudaError_t launch_one(const WRowParams<float>& p, int grid, size_t smem, cudaStream_t stream) {
+  auto kern = wrow2_kernel<WI, OP, P0>;
+  static bool configured[kMaxDevices] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!configured[dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMaxDynSmem);
+    if (e != cudaSuccess) return e;
+    configured[dev] = true;
+  }
+  kern<<<grid, 128, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+using Fn = cudaError_t (*)(const WRowParams<float>&, int, size_t, cudaStream_t);
+
+template <int WI, int P0>
+Fn by_op(int op) {
+  switch (op) {
+    case 0: return launch_one<WI, 0, P0>;
+    case 1: return launch_one<WI, 1, P0>;
+    case 2: return launch_one<WI, 2, P0>;
+    default: return launch_one<WI, 3, P0>;
+  }
+}
+
+template <int P0>
+Fn by_wavelet(int wi, int op) {
+  switch (wi) {
+    case 2: return by_op<2, P0>(op);
+    case 4: return by_op<4, P0>(op);
+    case 33: return by_op<33, P0>(op);
+    default: return nullptr;
+  }
+}
+
+}  // namespace
+
+int wrow2_levels_f32(int wi, int op, int p0) {
+  if (wi != 2 && wi != 4 && wi != 33) return 0;
+  if (p0 != 16 && p0 != 32) return 0;
+  return reg_max_levels(wi, op, p0);
+}
+
+cudaError_t launch_wrow2_f32(int wi, int op, int p0, const WRowParams<float>& p, int grid,
+                             size_t smem, cudaStream_t stream) {
+  Fn fn = p0 == 16 ? by_wavelet<16>(wi, op) : (p0 == 32 ? by_wavelet<32>(wi, op) : nullptr);
+  if (!fn) return cudaErrorInvalidValue;
+  return fn(p, grid, smem, stream);
+}
+
+int wrow2_resident_ctas(int p0) {
+  // shared memory bounds residency: two row slots, two buffers each
+  const size_t smem = (size_t)4 * 128 * p0 * sizeof(float) + 256;
+  const int per_sm = (int)((227 * 1024) / smem);
+  return per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
+}
+
+}  // namespace lw

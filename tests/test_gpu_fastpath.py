@@ -40,7 +40,7 @@ def run(x, w, tf, bc, axes, levels, fast=True):
 def test_rows_whole_line(dtype):
     rng = np.random.default_rng(21)
     for w in WAVELETS:
-        for n in (32, 64, 256, 1024, 4096):
+        for n in (32, 64, 256, 1024, 2048, 4096):
             for lv in (1, 2, 3, 5, 6, 9):
                 x = rng.standard_normal((3, n)).astype(dtype)
                 for tf in range(4):
@@ -123,3 +123,24 @@ def test_tma_strided_windows_and_whole_lines(op):
                 _lib.set_option("tma_strided", 1)
             assert np.array_equal(g, g2)
     assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
+
+
+def test_rows_two_warps_match_one_warp():
+    """float32 rows of 2048 and 4096 split over two warps equal the
+    one-warp-per-row kernel (option off) and the oracle."""
+    rng = np.random.default_rng(27)
+    for w in WAVELETS:
+        for n in (2048, 4096):
+            x = rng.standard_normal((5, n)).astype(np.float32)
+            for tf in range(4):
+                for lv in (1, 4, 6):
+                    rc, o = po.oracle_sep(x, w, tf, 0, [1], [lv])
+                    if rc:
+                        continue
+                    g, _ = run(x, w, tf, 0, [1], [lv])
+                    _lib.set_option("wrow_split", 0)
+                    try:
+                        g2, _ = run(x, w, tf, 0, [1], [lv])
+                    finally:
+                        _lib.set_option("wrow_split", 1)
+                    assert np.array_equal(g, o) and np.array_equal(g2, o), (w, n, tf, lv)
