@@ -354,6 +354,27 @@ def autograd_section(dev, steps: int = 10):
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
+    f64 = None
+    v64 = v.double()
+    g64 = gy.double()
+    x64 = v64.clone().requires_grad_(True)
+    t64 = []
+    for k in range(5):
+        a, b, c = ev(), ev(), ev()
+        x64.grad = None
+        a.record()
+        y64 = ag.dwt(x64, "db4", "Zero", axes=(0, 1, 2), level=(4, 4, 4))
+        b.record()
+        y64.backward(g64)
+        c.record()
+        torch.cuda.synchronize(dev)
+        if k >= 2:
+            t64.append((a.elapsed_time(b), b.elapsed_time(c)))
+    f64 = {"forward_ms": round(float(np.median([u for u, _ in t64])), 4),
+           "backward_ms": round(float(np.median([w for _, w in t64])), 4)}
+    f64["forward_gbs"] = round(2 * v64.numel() * 8 / f64["forward_ms"] / 1e6, 1)
+    del v64, g64, x64, y64
+
     fw, bw, plain = [], [], []
     for k in range(steps + 2):
         a, b, c, d, e = ev(), ev(), ev(), ev(), ev()
@@ -377,7 +398,8 @@ def autograd_section(dev, steps: int = 10):
             "forward_ms": round(f, 4), "backward_ms": round(bk, 4),
             "plain_forward_ms": round(pln, 4),
             "backward_over_forward": round(bk / f, 3),
-            "forward_gbs": round(B / f / 1e6, 1), "backward_gbs": round(B / bk / 1e6, 1)}
+            "forward_gbs": round(B / f / 1e6, 1), "backward_gbs": round(B / bk / 1e6, 1),
+            "float64": f64}
 
 
 def lsq_section(dev, steps: int = 200, check_steps: int = 3):

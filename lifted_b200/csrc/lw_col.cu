@@ -9,9 +9,9 @@
 namespace lw {
 namespace {
 
-template <int WI, int OP, int V>
-cudaError_t launch_one(const ColParams& p, int grid, size_t smem, cudaStream_t stream) {
-  auto kern = col_kernel<WI, OP, V>;
+template <typename T, int WI, int OP, int V>
+cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_t stream) {
+  auto kern = col_kernel<T, WI, OP, V>;
   static bool configured[kMaxDevices] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -27,35 +27,36 @@ cudaError_t launch_one(const ColParams& p, int grid, size_t smem, cudaStream_t s
   return cudaGetLastError();
 }
 
-template <int WI, int V>
-ColFn by_op(int op) {
+template <typename T, int WI, int V>
+ColFn<T> by_op(int op) {
   switch (op) {
-    case 0: return launch_one<WI, 0, V>;
-    case 1: return launch_one<WI, 1, V>;
-    case 2: return launch_one<WI, 2, V>;
-    default: return launch_one<WI, 3, V>;
+    case 0: return launch_one<T, WI, 0, V>;
+    case 1: return launch_one<T, WI, 1, V>;
+    case 2: return launch_one<T, WI, 2, V>;
+    default: return launch_one<T, WI, 3, V>;
   }
 }
 
-template <int V>
-ColFn by_wavelet(int wi, int op) {
+template <typename T, int V>
+ColFn<T> by_wavelet(int wi, int op) {
   switch (wi) {
-    case 2: return by_op<2, V>(op);
-    case 4: return by_op<4, V>(op);
-    case 33: return by_op<33, V>(op);
+    case 2: return by_op<T, 2, V>(op);
+    case 4: return by_op<T, 4, V>(op);
+    case 33: return by_op<T, 33, V>(op);
     default: return nullptr;
   }
 }
 
 }  // namespace
 
-ColFn pick_col(int wi, int op, int v) {
-  return v == 2 ? by_wavelet<2>(wi, op) : by_wavelet<1>(wi, op);
+ColFn<float> pick_col_f32(int wi, int op, int v) {
+  return v == 2 ? by_wavelet<float, 2>(wi, op) : by_wavelet<float, 1>(wi, op);
 }
+ColFn<double> pick_col_f64(int wi, int op) { return by_wavelet<double, 1>(wi, op); }
 
-size_t col_smem_bytes(int hmax, int v) {
-  return (size_t)COL_ROWS * COL_LANES * v * sizeof(float) +
-         (size_t)4 * hmax * COL_THREADS * v * sizeof(float) + 16;
+size_t col_smem_bytes(int hmax, int v, int elem_bytes) {
+  return (size_t)COL_ROWS * COL_LANES * v * elem_bytes +
+         (size_t)4 * hmax * COL_THREADS * v * elem_bytes + 16;
 }
 
 }  // namespace lw

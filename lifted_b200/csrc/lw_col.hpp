@@ -7,13 +7,16 @@
 
 namespace lw {
 
+template <typename T>
 struct ColParams;
-using ColFn = cudaError_t (*)(const ColParams&, int, size_t, cudaStream_t);
+template <typename T>
+using ColFn = cudaError_t (*)(const ColParams<T>&, int, size_t, cudaStream_t);
 
 // Launcher for (catalogue wavelet, transform, lines per lane); nullptr if
-// not compiled.
-ColFn pick_col(int wi, int op, int v);
+// not compiled.  float64 has one line per lane only.
+ColFn<float> pick_col_f32(int wi, int op, int v);
+ColFn<double> pick_col_f64(int wi, int op);
 // Dynamic shared memory of one CTA: staging buffer, mailbox, mbarrier.
-size_t col_smem_bytes(int hmax, int v);
+size_t col_smem_bytes(int hmax, int v, int elem_bytes);
 
 }  // namespace lw

@@ -1,4 +1,4 @@
-// Persistent TMA-staged kernel for strided axes (float32): the first k
+// Persistent TMA-staged kernel for strided axes (float32, float64): the first k
 // levels of an axis pass on windows of 512 samples x 32*V adjacent lines.
 //
 // The lines of a strided axis pass are columns of a 2D (or 3D) view whose
@@ -19,8 +19,11 @@
 //                     those reads (level 2), so the next tile's copy overlaps
 //                     the two finest levels.
 //
-// With V = 2 a lane holds two adjacent lines and every step runs on packed
-// FP32x2 arithmetic (lw_reg_kernel.cuh, LaneVec), halving the instructions.
+// With V = 2 (float32) a lane holds two adjacent lines and every step runs on
+// packed FP32x2 arithmetic (lw_reg_kernel.cuh, LaneVec), halving the
+// instructions.  float64 runs with V = 1 and reads d_1 from the staging
+// buffer at the finest level (its registers hold no preloaded copy), so its
+// reverse passes release the buffer one level later.
 // The lifting arithmetic, the mailbox neighbour exchange and the band
 // stores are those of the register-blocked kernel in tile mode: interior
 // results are exact, the halo absorbs the corrupted window margins,
@@ -42,13 +45,14 @@ constexpr int COL_ROWS = 2 * COL_P0 * COL_CHUNKS;      // 512 window samples
 constexpr int COL_THREADS = COL_LANES * COL_CHUNKS;    // 512
 constexpr int COL_MAXK = 5;                            // levels per tile launch
 
+template <typename T>
 struct ColParams {
   // tm_rows[i]: the input viewed as {lines (x), axis (y)[, outer (z)]},
   // box {32*V, 256 >> i[, 1]}; tm_tmp: the approximation band buffer
   // [position][line], box {32*V, 512 >> k}.
   CUtensorMap tm_rows[COL_MAXK];
   CUtensorMap tm_tmp;
-  RegParams<float> r;   // geometry, program, tile, band buffer, levels
+  RegParams<T> r;       // geometry, program, tile, band buffer, levels
   int64_t ncols;        // lines along x (multiple of 32*V)
   int64_t nouter;       // z extent (1 for a 2D view)
   int64_t ntr;          // row tiles per strip
@@ -114,8 +118,8 @@ struct TileCoord {
   int64_t outer, col0, rt, wstart;
 };
 
-template <int V>
-__device__ __forceinline__ TileCoord decode(const ColParams& p, int64_t t) {
+template <typename T, int V>
+__device__ __forceinline__ TileCoord decode(const ColParams<T>& p, int64_t t) {
   const int64_t nstrips = p.ncols / (COL_LANES * V);
   const int64_t per_outer = nstrips * p.ntr;
   TileCoord c;
@@ -129,15 +133,15 @@ __device__ __forceinline__ TileCoord decode(const ColParams& p, int64_t t) {
 }
 
 // Issues the TMA copies of tile t into the staging buffer (one thread).
-template <bool FWD, int V>
-__device__ __forceinline__ void issue(const ColParams& p, int64_t t, float* stage,
+template <typename T, bool FWD, int V>
+__device__ __forceinline__ void issue(const ColParams<T>& p, int64_t t, T* stage,
                                       uint64_t* bar) {
-  constexpr int W = COL_LANES * V;  // floats per staging row
-  const TileCoord tc = decode<V>(p, t);
+  constexpr int W = COL_LANES * V;  // elements per staging row
+  const TileCoord tc = decode<T, V>(p, t);
   const int x = (int)tc.col0, z = (int)tc.outer;
   const bool r3 = p.rank3 != 0;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_expect(bar, COL_ROWS * W * sizeof(float));
+  mbar_expect(bar, COL_ROWS * W * sizeof(T));
   if (FWD) {
     tma_box(stage, &p.tm_rows[0], x, (int)tc.wstart, z, r3, bar);
     tma_box(stage + 256 * W, &p.tm_rows[0], x, (int)tc.wstart + 256, z, r3, bar);
@@ -163,10 +167,11 @@ __device__ __forceinline__ void issue(const ColParams& p, int64_t t, float* stag
 
 // Per-tile state of the reverse levels: where the staged bands are and how
 // to hand the buffer back.
+template <typename T>
 struct RevStage {
-  const float* stage;
+  const T* stage;
   uint64_t* bar;
-  const ColParams* p;
+  const ColParams<T>* p;
   int64_t next;  // next tile of this CTA (>= ntiles: none)
 };
 
@@ -174,45 +179,56 @@ struct RevStage {
 // (detail bands d_1.., region sizes 256, 128, ...) or of a_k (LV = k - 1).
 __device__ __forceinline__ int region_row(int lv) { return COL_ROWS - (COL_ROWS >> lv); }
 
-template <typename VT, int V, int P, int PA>
-__device__ __forceinline__ void read_rows(VT (&v)[PA], const float* stage, int row0, int lane) {
+template <typename T, typename VT, int V, int P, int PA>
+__device__ __forceinline__ void read_rows(VT (&v)[PA], const T* stage, int row0, int lane) {
   constexpr int W = COL_LANES * V;
-  const float* q = stage + (size_t)row0 * W + lane * V;
+  const T* q = stage + (size_t)row0 * W + lane * V;
 #pragma unroll
   for (int i = 0; i < P; ++i) v[i] = *reinterpret_cast<const VT*>(q + (size_t)i * W);
 }
 
-template <int WI, int OP, int P0, int HMAX, int V, int LV>
-__device__ __forceinline__ void rev_levels(typename LaneVec<float, V>::type (&s)[P0],
-                                           typename LaneVec<float, V>::type (&d)[P0],
-                                           const typename LaneVec<float, V>::type (&d1)[P0],
-                                           reg::Ctx<float>& c, const RevStage& rs) {
-  using VT = typename LaneVec<float, V>::type;
+// Whether the reverse levels keep d_1 in registers from the start (float32)
+// or read it from the staging buffer at the finest level (float64, whose
+// registers hold no room for the copy).
+template <typename T>
+constexpr bool preload_d1() {
+  return sizeof(T) == 4;
+}
+
+template <typename T, int WI, int OP, int P0, int HMAX, int V, int LV>
+__device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0],
+                                           typename LaneVec<T, V>::type (&d)[P0],
+                                           const typename LaneVec<T, V>::type (&d1)[P0],
+                                           reg::Ctx<T>& c, const RevStage<T>& rs) {
+  using VT = typename LaneVec<T, V>::type;
   constexpr int P = P0 >> LV;
+  // the level after whose reads the staging buffer is free
+  constexpr int LAST_READ = preload_d1<T>() ? 1 : 0;
   if constexpr (LV >= 0) {
     if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
       const int k = c.p->nreg;
       if (LV < k) {
-        const RegParams<float>& p = *c.p;
+        const RegParams<T>& p = *c.p;
         const int64_t nb = c.n >> (LV + 1);
         const int64_t gp0 = c.e0 >> (LV + 1);
-        if constexpr (LV > 0) {
-          if (LV + 1 == k) read_rows<VT, V, P, P0>(s, rs.stage, region_row(k) + c.r * P, c.j);
-          read_rows<VT, V, P, P0>(d, rs.stage, region_row(LV) + c.r * P, c.j);
-          if (LV == 1) {
-            // last read of the staging buffer for this tile
-            __syncthreads();
-            if (c.tid == 0 && rs.next < rs.p->ntiles)
-              issue<false, V>(*rs.p, rs.next, const_cast<float*>(rs.stage), rs.bar);
-          }
+        if (LV + 1 == k && (LV > 0 || !preload_d1<T>()))
+          read_rows<T, VT, V, P, P0>(s, rs.stage, region_row(k) + c.r * P, c.j);
+        if constexpr (LV > 0 || !preload_d1<T>()) {
+          read_rows<T, VT, V, P, P0>(d, rs.stage, region_row(LV) + c.r * P, c.j);
         } else {
 #pragma unroll
           for (int i = 0; i < P0; ++i) d[i] = d1[i];
         }
-        reg::steps<float, VT, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
+        if (LV == LAST_READ) {
+          // last read of the staging buffer for this tile
+          __syncthreads();
+          if (c.tid == 0 && rs.next < rs.p->ntiles)
+            issue<T, false, V>(*rs.p, rs.next, const_cast<T*>(rs.stage), rs.bar);
+        }
+        reg::steps<T, VT, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
         if constexpr (LV == 0) {
           if (reg::chunk_stored(c)) {
-            float* o = p.out + c.bout + c.e0 * p.g.sout;
+            T* o = p.out + c.bout + c.e0 * p.g.sout;
 #pragma unroll
             for (int i = 0; i < P; ++i) {
               *reinterpret_cast<VT*>(o + (2 * i) * p.g.sout) = s[i];
@@ -227,30 +243,31 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<float, V>::type (&s)
           }
         }
       }
-      if constexpr (LV > 0) rev_levels<WI, OP, P0, HMAX, V, LV - 1>(s, d, d1, c, rs);
+      if constexpr (LV > 0) rev_levels<T, WI, OP, P0, HMAX, V, LV - 1>(s, d, d1, c, rs);
     } else if constexpr (LV > 0) {
-      rev_levels<WI, OP, P0, HMAX, V, LV - 1>(s, d, d1, c, rs);
+      rev_levels<T, WI, OP, P0, HMAX, V, LV - 1>(s, d, d1, c, rs);
     }
   }
 }
 
 }  // namespace col
 
-template <int WI, int OP, int V>
+template <typename T, int WI, int OP, int V>
 __global__ void __launch_bounds__(COL_THREADS, 1)
-    col_kernel(const __grid_constant__ ColParams p) {
-  using VT = typename LaneVec<float, V>::type;
+    col_kernel(const __grid_constant__ ColParams<T> p) {
+  using VT = typename LaneVec<T, V>::type;
+  static_assert(V == 1 || sizeof(T) == 4, "packed lanes are float32 only");
   constexpr int P0 = COL_P0;
   constexpr int W = COL_LANES * V;
   constexpr int HMAX = cat_reach(WI, OP) > 0 ? cat_reach(WI, OP) : 1;
   constexpr bool FWD = (OP == TF_F || OP == TF_IA);
   extern __shared__ __align__(128) unsigned char col_smem[];
-  float* stage = reinterpret_cast<float*>(col_smem);
-  float* mbox = stage + COL_ROWS * W;
+  T* stage = reinterpret_cast<T*>(col_smem);
+  T* mbox = stage + COL_ROWS * W;
   uint64_t* bar = reinterpret_cast<uint64_t*>(mbox + 4 * HMAX * COL_THREADS * V);
 
   const int tid = threadIdx.x;
-  reg::Ctx<float> c;
+  reg::Ctx<T> c;
   c.p = &p.r;
   c.nth = COL_THREADS;
   c.tid = tid;
@@ -269,7 +286,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   __syncthreads();
   uint32_t parity = 0;
   int64_t t = blockIdx.x;
-  if (t < p.ntiles && tid == 0) col::issue<FWD, V>(p, t, stage, bar);
+  if (t < p.ntiles && tid == 0) col::issue<T, FWD, V>(p, t, stage, bar);
   for (; t < p.ntiles; t += gridDim.x) {
     const bool got = col::mbar_wait(bar, parity, p.spin_limit);
     if (!__syncthreads_and(got)) {
@@ -278,7 +295,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
       return;
     }
     parity ^= 1;
-    const col::TileCoord tc = col::decode<V>(p, t);
+    const col::TileCoord tc = col::decode<T, V>(p, t);
     const int64_t L = tc.outer * p.ncols + tc.col0 + (int64_t)c.j * V;
     c.L = L;
     c.line_ok = L < p.r.g.nlines;  // V lines together (ncols % (32 V) == 0)
@@ -293,27 +310,34 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
 
     VT s[P0], d[P0];
     if constexpr (FWD) {
-      const float* st = stage + (size_t)(c.r * 2 * P0) * W + c.j * V;
+      const T* st = stage + (size_t)(c.r * 2 * P0) * W + c.j * V;
 #pragma unroll
       for (int i = 0; i < P0; ++i) {
         s[i] = *reinterpret_cast<const VT*>(st + (size_t)(2 * i) * W);
         d[i] = *reinterpret_cast<const VT*>(st + (size_t)(2 * i + 1) * W);
       }
       __syncthreads();  // staging consumed
-      if (tid == 0 && next < p.ntiles) col::issue<FWD, V>(p, next, stage, bar);
-      reg::fwd_levels<float, VT, V, WI, OP, P0, HMAX, 0, true>(s, d, c);
+      if (tid == 0 && next < p.ntiles) col::issue<T, FWD, V>(p, next, stage, bar);
+      reg::fwd_levels<T, VT, V, WI, OP, P0, HMAX, 0, true>(s, d, c);
     } else {
       const int k = p.r.nreg;
-      VT d1[P0];
-      col::read_rows<VT, V, P0, P0>(d1, stage, c.r * P0, c.j);  // d_1 region
-      if (k == 1) {
-        col::read_rows<VT, V, P0, P0>(s, stage, col::region_row(1) + c.r * P0, c.j);
-        __syncthreads();
-        if (tid == 0 && next < p.ntiles) col::issue<FWD, V>(p, next, stage, bar);
+      VT d1[col::preload_d1<T>() ? P0 : 1];
+      if constexpr (col::preload_d1<T>()) {
+        col::read_rows<T, VT, V, P0, P0>(d1, stage, c.r * P0, c.j);  // d_1 region
+        if (k == 1) {
+          col::read_rows<T, VT, V, P0, P0>(s, stage, col::region_row(1) + c.r * P0, c.j);
+          __syncthreads();
+          if (tid == 0 && next < p.ntiles) col::issue<T, FWD, V>(p, next, stage, bar);
+        }
       }
-      col::RevStage rs{stage, bar, &p, next};
+      col::RevStage<T> rs{stage, bar, &p, next};
       constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
-      col::rev_levels<WI, OP, P0, HMAX, V, TOP>(s, d, d1, c, rs);
+      if constexpr (col::preload_d1<T>()) {
+        col::rev_levels<T, WI, OP, P0, HMAX, V, TOP>(s, d, d1, c, rs);
+      } else {
+        VT dummy[P0];
+        col::rev_levels<T, WI, OP, P0, HMAX, V, TOP>(s, d, dummy, c, rs);
+      }
     }
   }
 }

@@ -399,12 +399,14 @@ EncodeTiledFn encode_tiled_fn() {
 }
 
 bool encode_rows(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims,
-                 const cuuint64_t* strides, cuuint32_t box_x, cuuint32_t box_y) {
+                 const cuuint64_t* strides, cuuint32_t box_x, cuuint32_t box_y,
+                 int elem_bytes) {
   EncodeTiledFn enc = encode_tiled_fn();
   if (!enc) return false;
   const cuuint32_t box[3] = {box_x, box_y, 1};
   const cuuint32_t es[3] = {1, 1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<void*>(base),
+  return enc(m, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+             (cuuint32_t)rank, const_cast<void*>(base),
              dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -419,16 +421,15 @@ int band_pass(const RegPassArgs<T>& a, const LineGeom& g2, const T* in, T* out, 
 // approximation band.  Returns 0 when the pass does not qualify.
 template <typename T>
 int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
-  if constexpr (sizeof(T) != 4) {
-    return 0;
-  } else {
+  {
+    constexpr int EB = (int)sizeof(T);
     const LineGeom& g = a.g;
     if (!col_enabled()) return 0;
-    if (g.sin <= 1 || ((g.sin * 4) & 15)) return 0;
+    if (g.sin <= 1 || ((g.sin * EB) & 15)) return 0;
     if (!lines_adjacent(g) || g.nother > 2) return 0;
     const int64_t ncols = g.oshape[0];
     if (ncols % COL_LANES) return 0;
-    if (g.nother == 2 && (g.oin[1] <= 0 || ((g.oin[1] * 4) & 15))) return 0;
+    if (g.nother == 2 && (g.oin[1] <= 0 || ((g.oin[1] * EB) & 15))) return 0;
     if (!aligned16(a.in)) return 0;
     const int64_t n = g.n;
     if (n % 32) return 0;
@@ -436,7 +437,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // two adjacent lines per lane (packed FP32x2) when the line groups and
     // every line base of the output stay 8-byte aligned
     int v = 1;
-    if (col_packed() && ncols % (2 * COL_LANES) == 0 && (g.sout % 2) == 0 &&
+    if (EB == 4 && col_packed() && ncols % (2 * COL_LANES) == 0 && (g.sout % 2) == 0 &&
         (g.nother < 2 || (g.oout[1] % 2) == 0) && (reinterpret_cast<uintptr_t>(a.out) & 7) == 0)
       v = 2;
     const int maxreg = std::min(reg_max_levels(wi, op, COL_P0), COL_MAXK);
@@ -466,7 +467,9 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // packed lanes only while they still give every SM a tile
     if (v == 2 && ncols / (2 * COL_LANES) * ntr * (g.nother == 2 ? g.oshape[1] : 1) < sm_count())
       v = 1;
-    ColFn fn = pick_col(wi, op, v);
+    ColFn<T> fn;
+    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wi, op, v);
+    else fn = pick_col_f64(wi, op);
     if (!fn) return 0;
     const int64_t m = n >> k;
     const bool more = a.levels > k;
@@ -480,21 +483,21 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       cudaError_t e = scratch_alloc((void**)&tmp, (size_t)g.nlines * m * sizeof(T), stream);
       if (e != cudaSuccess) return -(int)e - 1000;
     }
-    ColParams cp;
+    ColParams<T> cp;
     std::memset(&cp, 0, sizeof(cp));
     const int rank = g.nother == 2 ? 3 : 2;
     const cuuint64_t dims[3] = {(cuuint64_t)ncols, (cuuint64_t)n,
                                 (cuuint64_t)(g.nother == 2 ? g.oshape[1] : 1)};
-    const cuuint64_t strides[2] = {(cuuint64_t)g.sin * 4,
-                                   (cuuint64_t)(g.nother == 2 ? g.oin[1] : 0) * 4};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.sin * EB,
+                                   (cuuint64_t)(g.nother == 2 ? g.oin[1] : 0) * EB};
     bool ok = true;
     const cuuint32_t bx = (cuuint32_t)(COL_LANES * v);
     for (int i = 0; i < k && ok; ++i)
-      ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, bx, (cuuint32_t)(256 >> i));
+      ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, bx, (cuuint32_t)(256 >> i), EB);
     if (ok && more) {
       const cuuint64_t tdims[2] = {(cuuint64_t)g.nlines, (cuuint64_t)m};
-      const cuuint64_t tstr[1] = {(cuuint64_t)g.nlines * 4};
-      ok = encode_rows(&cp.tm_tmp, tmp, 2, tdims, tstr, bx, (cuuint32_t)(COL_ROWS >> k));
+      const cuuint64_t tstr[1] = {(cuuint64_t)g.nlines * EB};
+      ok = encode_rows(&cp.tm_tmp, tmp, 2, tdims, tstr, bx, (cuuint32_t)(COL_ROWS >> k), EB);
     }
     if (!ok) {
       if (tmp) scratch_free(tmp, stream);
@@ -524,7 +527,11 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     cp.spin_limit = 1 << 22;
     cp.err = err;
     const int hmax = cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1;
-    const size_t smem = col_smem_bytes(hmax, v);
+    const size_t smem = col_smem_bytes(hmax, v, EB);
+    if (smem > kMaxDynSmem) {
+      if (tmp) scratch_free(tmp, stream);
+      return 0;
+    }
     const int grid = (int)std::min<int64_t>(cp.ntiles, sm_count());
 
     // band geometry: one other dim of nlines lines in tmp [position][line]

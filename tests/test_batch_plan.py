@@ -121,3 +121,29 @@ def test_invalid_batches_refused():
     p = BatchPlan([0, 3], [2, 4], [1, 0])
     assert p.info["nitems"] == 0
     p.close()
+
+
+def test_tuning_table_round_trip_and_use(tmp_path):
+    """A tuning entry for (wavelet, dtype, transform, log2 length) sets the
+    tile width and levels per group of later plans; the table survives a
+    save / load round trip as JSON."""
+    from lifted_b200 import batch as bt
+
+    bt.tune_clear()
+    path = tmp_path / "tune.json"
+    path.write_text('[\n  {"wavelet": 100907, "dtype_bytes": 4, "op": 0, "log2_length": 15, '
+                    '"stride": 1, "tile": 1024, "tile_levels": 2, "us": 12.5}\n]\n')
+    assert bt.tune_load(str(path)) == 1
+    plan = BatchPlan([40000], [100907], [6], op=0, dtype="float32")
+    items = plan.items()
+    f = {k: i for i, k in enumerate(ITEM_FIELDS)}
+    tiles = items[np.isin(items[:, f["kind"]], [2, 3])]
+    assert len(tiles) > 0
+    assert set(tiles[:, f["nlev"]].tolist()) <= {1, 2}
+    assert (tiles[:, f["t1"]] - tiles[:, f["t0"]]).max() == 1024
+    plan.close()
+    out = tmp_path / "saved.json"
+    bt.tune_save(str(out))
+    bt.tune_clear()
+    assert bt.tune_load(str(out)) == 1
+    bt.tune_clear()

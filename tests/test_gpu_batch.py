@@ -93,3 +93,27 @@ def test_oneshot_c_abi_and_checks():
     rc = lib.lifted_lwt_batch_f32(0, 0, n, ctypes.byref(tab), x.ctypes.data,
                                   yt.data_ptr(), stream)
     assert rc == _lib.EINVAL
+
+
+def test_autotuner_records_a_choice_that_plans_use(tmp_path):
+    """The autotuner times (tile width, levels per group) candidates on the
+    GPU for a wavelet and length, records the fastest, and later plans with
+    that key use it; results stay exact."""
+    from lifted_b200 import batch as bt
+
+    bt.tune_clear()
+    bt.autotune(["cdf9.7", "db4"], 1 << 15, op=0, total=1 << 21)
+    path = tmp_path / "tune.json"
+    bt.tune_save(str(path))
+    text = path.read_text()
+    assert '"wavelet": 100907' in text and '"wavelet": 4' in text
+    rng = np.random.default_rng(5)
+    lengths = [1 << 15, 30000, 1 << 15]
+    ws = [100907, 4, 100907]
+    lv = [5, 4, 6]
+    x = rng.standard_normal(sum(lengths)).astype(np.float32)
+    plan = BatchPlan(lengths, ws, lv, op=0, dtype="float32")
+    got = run_plan(plan, x)
+    assert np.array_equal(got, oracle_batch(x, lengths, ws, lv, 0, 0))
+    plan.close()
+    bt.tune_clear()

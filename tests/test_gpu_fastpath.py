@@ -98,8 +98,9 @@ def test_other_boundaries_fall_back_exactly():
             assert rc == 0 and np.array_equal(g, o), (bc, tf)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("op", [0, 1, 2, 3])
-def test_tma_strided_windows_and_whole_lines(op):
+def test_tma_strided_windows_and_whole_lines(op, dtype):
     """Strided float32 passes on the TMA-staged kernel (line counts that are
     multiples of 32): 2D columns with 512-sample windows and halos, whole
     lines up to 512, a 3D view (rank-3 tensor maps), in place; bit for bit
@@ -110,7 +111,7 @@ def test_tma_strided_windows_and_whole_lines(op):
              ((96, 64), [1, 0], [2, 5])]
     for w in WAVELETS:
         for shape, axes, lv in cases:
-            x = rng.standard_normal(shape).astype(np.float32)
+            x = rng.standard_normal(shape).astype(dtype)
             rc, o = po.oracle_sep(x, w, op, 0, axes, lv)
             if rc:
                 continue
