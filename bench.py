@@ -289,6 +289,40 @@ def batched_section(dev, plain_sample: int = 300, steps: int = 5):
             "speedup_vs_plain": round(gbs / plain_gbs, 1)}
 
 
+def inverse_section(dev, x, steps: int = 10):
+    """Inverse + InverseAdjoint of the headline workload (the same kernels
+    with the step order and signs of those transforms), timed as a CUDA
+    graph replay on the already-resident image."""
+    import torch
+    from lifted_b200 import pylifted as pl
+
+    w = torch.empty_like(x)
+    y = torch.empty_like(x)
+
+    def step():
+        pl._lwt(x, WAVELET, BC, 1, AXES, LEVELS, 1, out=w)
+        pl._lwt(w, WAVELET, BC, 3, AXES, LEVELS, 1, out=y)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize(dev)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+        step()
+    graph.replay()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    return {"workload": "as the headline, Inverse + InverseAdjoint (L2 not flushed between "
+                        "replays)", "value": round(BYTES_PER_STEP / ms / 1e6, 3), "unit": "GB/s",
+            "ms_per_step": round(ms, 4)}
+
+
 def cfg1_section(dev, steps: int = 10):
     """Plain 1D float64: 64 signals of 65536 i.i.d. N(0,1) (seed 1001),
     Daubechies2, 5 levels along axis 1, Zero boundary, Forward then
@@ -629,8 +663,10 @@ def main() -> int:
                              f"(reference sources + Highway stand-in, {variant}, "
                              f"{cores} threads)"}
 
-    extras = {"cfg1_1d_f64": None, "batched": None, "autograd": None, "lsq": None}
+    extras = {"inverse": None, "cfg1_1d_f64": None, "batched": None, "autograd": None,
+              "lsq": None}
     if world == 1 and not args.no_extras:
+        extras["inverse"] = inverse_section(dev, x)
         extras["cfg1_1d_f64"] = cfg1_section(dev)
         extras["batched"] = batched_section(dev)
         extras["autograd"] = autograd_section(dev)
@@ -663,6 +699,7 @@ def main() -> int:
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "inverse": extras["inverse"],
             "cfg1_1d_f64": extras["cfg1_1d_f64"],
             "batched": extras["batched"],
             "autograd": extras["autograd"],
