@@ -128,6 +128,19 @@ __device__ __forceinline__ void tile_step(const DevStep<T>& st, T* S, T* D,
       }
       Y[q] = y;
     }
+  } else if (st.kind == K_REPEAT && nt == 2) {
+    const T c0 = sub ? -st.c[0] : st.c[0];
+    for (int q = tid; q < nyw; q += nth) {
+      const int b = q + off;
+      T x0;
+      if (b >= 0 && b + 2 <= xhi) {
+        x0 = X[b] + X[b + 1];
+      } else {
+        x0 = (b >= 0 && b < xhi) ? X[b] : T(0);
+        if (b + 1 >= 0 && b + 1 < xhi) x0 += X[b + 1];
+      }
+      Y[q] = fop(0, c0, x0, Y[q]);
+    }
   } else if (st.kind == K_REPEAT) {
     for (int q = tid; q < nyw; q += nth) {
       const int b = q + off;
@@ -205,14 +218,18 @@ __device__ void tile_fwd(const BatchParams<T>& p, const BatchItem& w,
     wl1 = gb + nsw;
     m = ns;
     if (j + 1 < w.nlev) {
-      for (int q = tid; q < nsw; q += nth) X[q] = S[q];
+      // split the approximation band in one pass: evens to X, odds to D
+      // (D was stored above), then X becomes S
       __syncthreads();
       for (int i = tid; i < nsw; i += nth) {
-        const T v = X[i];
+        const T v = S[i];
         if (i & 1) D[i >> 1] = v;
-        else S[i >> 1] = v;
+        else X[i >> 1] = v;
       }
       __syncthreads();
+      T* t = S;
+      S = X;
+      X = t;
     }
   }
   T* dst = band_ptr_w(p, w.dst_sel, w.dst_off);
