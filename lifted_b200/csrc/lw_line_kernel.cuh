@@ -164,6 +164,18 @@ __device__ void fold_back(const DevStep<T>& st, int bc, T* y, int64_t ny,
   }
 }
 
+// Line j and position i of flat index f over W lines of m elements (no
+// division for a single line).
+__device__ __forceinline__ void split_index(int64_t f, int64_t m, int W, int& j, int64_t& i) {
+  if (W == 1) {
+    j = 0;
+    i = f;
+  } else {
+    j = (int)(f / m);
+    i = f - (int64_t)j * m;
+  }
+}
+
 // One step over W lines held at A + j * pitch as [s (ns) | d (nd)].
 template <typename T>
 __device__ void run_step(const DevStep<T>& st, int normal, int across,
@@ -175,8 +187,9 @@ __device__ void run_step(const DevStep<T>& st, int normal, int across,
     const int64_t m = ns + nd;
     const int64_t tot = (int64_t)W * m;
     for (int64_t f = tid; f < tot; f += nth) {
-      int j = (int)(f / m);
-      int64_t i = f - (int64_t)j * m;
+      int j;
+      int64_t i;
+      split_index(f, m, W, j, i);
       T* p = A + j * pitch + i;
       *p = *p * (i < ns ? st.sm : st.dm);
     }
@@ -194,8 +207,9 @@ __device__ void run_step(const DevStep<T>& st, int normal, int across,
     // indices in both edge ranges get both updates, front first (Q5).
     const int64_t tot = (int64_t)W * ny;
     for (int64_t f = tid; f < tot; f += nth) {
-      int j = (int)(f / ny);
-      int64_t i = f - (int64_t)j * ny;
+      int j;
+      int64_t i;
+      split_index(f, ny, W, j, i);
       T* line = A + j * pitch;
       const T* x = line + xo;
       T y = line[yo + i];
@@ -220,8 +234,9 @@ __device__ void run_step(const DevStep<T>& st, int normal, int across,
     if (hi > 0) {
       const int64_t tot = (int64_t)W * hi;
       for (int64_t f = tid; f < tot; f += nth) {
-        int j = (int)(f / hi);
-        int64_t i = f - (int64_t)j * hi;
+        int j;
+        int64_t i;
+        split_index(f, hi, W, j, i);
         T* line = A + j * pitch;
         const T* x = line + xo;
         T y = line[yo + i];
@@ -243,8 +258,10 @@ __device__ void run_step(const DevStep<T>& st, int normal, int across,
     } else if (nback > 0) {
       const int64_t tot = (int64_t)W * nback;
       for (int64_t f = tid; f < tot; f += nth) {
-        int j = (int)(f / nback);
-        int64_t i = n2 + (f - (int64_t)j * nback);
+        int j;
+        int64_t i;
+        split_index(f, nback, W, j, i);
+        i += n2;
         T* line = A + j * pitch;
         line[yo + i] = ip_bc(st, BC_ZERO, line[yo + i], line + xo, nx, i);
       }
@@ -276,14 +293,16 @@ __device__ void coarse_forward(const DevProgram<T>& prog, int bc, T* A,
     const int64_t nd = m / 2, ns = m - nd;
     const int64_t t2 = (int64_t)W * m;
     for (int64_t f = tid; f < t2; f += nth) {
-      int j = (int)(f / m);
-      int64_t i = f - (int64_t)j * m;
+      int j;
+      int64_t i;
+      split_index(f, m, W, j, i);
       B[j * pitch_b + i] = A[j * pitch + i];
     }
     __syncthreads();
     for (int64_t f = tid; f < t2; f += nth) {
-      int j = (int)(f / m);
-      int64_t i = f - (int64_t)j * m;
+      int j;
+      int64_t i;
+      split_index(f, m, W, j, i);
       A[j * pitch + ((i & 1) ? ns + (i >> 1) : (i >> 1))] = B[j * pitch_b + i];
     }
     __syncthreads();
@@ -312,14 +331,16 @@ __device__ void coarse_reverse(const DevProgram<T>& prog, int bc, T* A,
     run_program(prog, bc, A, pitch, W, ns, nd);
     const int64_t t2 = (int64_t)W * m;
     for (int64_t f = tid; f < t2; f += nth) {
-      int j = (int)(f / m);
-      int64_t i = f - (int64_t)j * m;
+      int j;
+      int64_t i;
+      split_index(f, m, W, j, i);
       B[j * pitch_b + i] = A[j * pitch + i];
     }
     __syncthreads();
     for (int64_t f = tid; f < t2; f += nth) {
-      int j = (int)(f / m);
-      int64_t i = f - (int64_t)j * m;
+      int j;
+      int64_t i;
+      split_index(f, m, W, j, i);
       int64_t src = (i & 1) ? ns + (i >> 1) : (i >> 1);
       A[j * pitch + i] = B[j * pitch_b + src];
     }
