@@ -176,6 +176,31 @@ def cpu_reference_time(img: np.ndarray, budget_s: float, min_steps: int = 1):
     return el / steps, steps, cores, variant
 
 
+def cpu_ref_sample(run_once, bytes_per_run: float, budget_s: float = 4.0):
+    """Times `run_once` (a call of the reference's CPU implementation) until
+    `budget_s` seconds have passed (at least once); returns a cpu_baseline
+    object or None when the reference build is missing."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    variant = po.best_ref_variant()
+    if variant is None:
+        return None
+    cores = po.nproc()
+    run_once(variant, cores)  # warm the thread pool
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        run_once(variant, cores)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    return {"value": round(bytes_per_run * n / el / 1e9, 3), "unit": "GB/s", "cores": cores,
+            "kind": "reference", "runs": n,
+            "sample": f"reference sources + Highway stand-in ({variant}), {cores} threads"}
+
+
 def run_reference_arm(args, rank: int) -> int:
     if rank != 0:
         return 0
@@ -272,6 +297,20 @@ def batched_section(dev, plain_sample: int = 300, steps: int = 5):
     torch.cuda.synchronize(dev)
     pel = time.perf_counter() - t0
     plain_gbs = 2 * 2 * samp * 4 / pel / 1e9
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    xh = x.cpu().numpy()
+    sig = [(xh[int(offs[i]):int(offs[i]) + int(lengths[i])], int(ws[i]), lv[i]) for i in idx]
+
+    def cpu_once(variant, cores):
+        for v, wv, l in sig:
+            rc, o = po.ref_sep(v, wv, 0, 0, [0], [l], variant=variant, nthreads=cores)
+            po.ref_sep(o, wv, 2, 0, [0], [l], variant=variant, nthreads=cores)
+
+    cpu = cpu_ref_sample(cpu_once, 2 * 2 * samp * 4)
+    if cpu is not None:
+        cpu["sample"] += f"; the {len(idx)} sampled signals, one call per signal and transform"
     pf.close()
     pa.close()
     gbs = bytes_step / ms / 1e6
@@ -286,7 +325,8 @@ def batched_section(dev, plain_sample: int = 300, steps: int = 5):
                                "sample": f"{len(idx)} random signals of the batch "
                                          f"({samp} samples), one C ABI call per signal "
                                          f"and transform, wall clock"},
-            "speedup_vs_plain": round(gbs / plain_gbs, 1)}
+            "speedup_vs_plain": round(gbs / plain_gbs, 1),
+            "cpu_reference": cpu}
 
 
 def inverse_section(dev, x, steps: int = 10):
@@ -361,10 +401,22 @@ def cfg1_section(dev, steps: int = 10):
     wtr = pl.lwt_forward_adjoint(r, "db2", "Zero", axes=(1,), level=(5,))
     a, b = float((wx * r).sum()), float((x * wtr).sum())
     B = 2 * 2 * x.numel() * 8
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    xh = x.cpu().numpy()
+    wh = np.empty_like(xh)
+    yh = np.empty_like(xh)
+
+    def cpu_once(variant, cores):
+        po.ref_sep(xh, 2, 0, 0, [1], [5], out=wh, variant=variant, nthreads=cores)
+        po.ref_sep(wh, 2, 2, 0, [1], [5], out=yh, variant=variant, nthreads=cores)
+
     return {"workload": "float64 64 x 65536 N(0,1) (seed 1001), Daubechies2, 5 levels on "
                         "axis 1, Zero boundary, Forward + ForwardAdjoint",
             "value": round(B / ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(ms, 4),
-            "dot_product_rel_err": abs(a - b) / abs(a)}
+            "dot_product_rel_err": abs(a - b) / abs(a),
+            "cpu_reference": cpu_ref_sample(cpu_once, B)}
 
 
 def autograd_section(dev, steps: int = 10):
@@ -427,13 +479,23 @@ def autograd_section(dev, steps: int = 10):
             plain.append(c.elapsed_time(d))
     f, bk, pln = float(np.median(fw)), float(np.median(bw)), float(np.median(plain))
     B = 2 * v.numel() * 4
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    vh = v.cpu().numpy()
+    oh = np.empty_like(vh)
+
+    def cpu_once(variant, cores):
+        po.ref_sep(vh, 4, 0, 0, [0, 1, 2], [4, 4, 4], out=oh, variant=variant, nthreads=cores)
+
+    cpu = cpu_ref_sample(cpu_once, B, budget_s=3.0)
     return {"workload": "3D float32 512^3 box-smoothed N(0,1) (seed 1003), Daubechies4, "
                         "levels (4,4,4), axes (0,1,2), Zero boundary",
             "forward_ms": round(f, 4), "backward_ms": round(bk, 4),
             "plain_forward_ms": round(pln, 4),
             "backward_over_forward": round(bk / f, 3),
             "forward_gbs": round(B / f / 1e6, 1), "backward_gbs": round(B / bk / 1e6, 1),
-            "float64": f64}
+            "float64": f64, "cpu_reference_forward": cpu}
 
 
 def lsq_section(dev, steps: int = 200, check_steps: int = 3):

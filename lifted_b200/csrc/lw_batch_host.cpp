@@ -41,6 +41,9 @@ struct lifted_batch_plan {
   int64_t max_in = 0, max_out = 0;  // highest element index + 1 touched
   // completion of the last run, so that a run on another stream starts after it
   cudaEvent_t last = nullptr;
+  // device buffers from the stream-ordered pool (plans the library caches
+  // for long lines), freed stream-ordered after the last run
+  bool pooled = false;
   // captured graph of one run and the pointers it was captured with
   cudaGraphExec_t gexec = nullptr;
   const void* g_in = nullptr;
@@ -466,7 +469,7 @@ int plan_create(uint32_t op, uint32_t bc, size_t nsig,
 // Binds the plan to the current device on its first run: launch shape from
 // the kernel's occupancy, device copies of the queue and programs, scratch.
 template <typename T>
-int ensure_device(lifted_batch_plan* p) {
+int ensure_device(lifted_batch_plan* p, cudaStream_t stream = nullptr) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
@@ -486,22 +489,31 @@ int ensure_device(lifted_batch_plan* p) {
                      "%zu bytes of shared memory", p->block, p->smem);
   p->grid = (int)std::min<int64_t>((int64_t)sms * occ, (int64_t)p->items.size());
   cudaError_t e;
-  e = cudaMalloc(&p->d_items, p->items.size() * sizeof(BatchItem));
-  if (e == cudaSuccess) e = cudaMalloc(&p->d_progs, p->progs_bytes);
-  if (e == cudaSuccess)
-    e = cudaMalloc((void**)&p->d_sync, (size_t)(2 + p->ncounters) * sizeof(int32_t));
-  if (e == cudaSuccess && p->scratch_bytes) e = cudaMalloc(&p->d_scratch, p->scratch_bytes);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(p->d_items, p->items.data(), p->items.size() * sizeof(BatchItem),
-                   cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(p->d_progs, p->progs_host.data(), p->progs_bytes, cudaMemcpyHostToDevice);
+  auto alloc = [&](void** ptr, size_t bytes) {
+    return p->pooled ? scratch_alloc(ptr, bytes, stream) : cudaMalloc(ptr, bytes);
+  };
+  auto upload = [&](void* dst, const void* src, size_t bytes) {
+    // pageable source: the call returns once the data is staged
+    return p->pooled ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream)
+                     : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  };
+  auto release = [&](void* ptr) {
+    if (!ptr) return;
+    if (p->pooled) scratch_free(ptr, stream);
+    else cudaFree(ptr);
+  };
+  e = alloc(&p->d_items, p->items.size() * sizeof(BatchItem));
+  if (e == cudaSuccess) e = alloc(&p->d_progs, p->progs_bytes);
+  if (e == cudaSuccess) e = alloc((void**)&p->d_sync, (size_t)(2 + p->ncounters) * sizeof(int32_t));
+  if (e == cudaSuccess && p->scratch_bytes) e = alloc(&p->d_scratch, p->scratch_bytes);
+  if (e == cudaSuccess) e = upload(p->d_items, p->items.data(), p->items.size() * sizeof(BatchItem));
+  if (e == cudaSuccess) e = upload(p->d_progs, p->progs_host.data(), p->progs_bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    cudaFree(p->d_items);
-    cudaFree(p->d_progs);
-    cudaFree(p->d_sync);
-    cudaFree(p->d_scratch);
+    release(p->d_items);
+    release(p->d_progs);
+    release(p->d_sync);
+    release(p->d_scratch);
     p->d_items = p->d_progs = p->d_scratch = nullptr;
     p->d_sync = nullptr;
     return set_error(e == cudaErrorMemoryAllocation ? LIFTED_ENOMEM : LIFTED_ECUDA,
@@ -528,7 +540,7 @@ int plan_run(lifted_batch_plan* p, const T* in, T* out, cudaStream_t stream,
   const char* oe = (const char*)(out + p->max_out);
   if (ib < oe && ob < ie)
     return set_error(LIFTED_EINVAL, "batch input and output overlap");
-  int rc = ensure_device<T>(p);
+  int rc = ensure_device<T>(p, stream);
   if (rc) return rc;
   // runs of one plan share its queue and counters: order them on the GPU
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -664,19 +676,22 @@ int run_lines_batched(uint32_t wavelet, int op, int bc, const LineGeom& g, int l
       sig[L].in_offset = (uint64_t)bi;
       sig[L].out_offset = (uint64_t)bo;
     }
+    // a new plan allocates: not inside a stream capture
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) cudaGetLastError();
+    if (cap != cudaStreamCaptureStatusNone) return 0;
     const int rc = plan_create<T>((uint32_t)op, (uint32_t)bc, sig.size(), sig.data(), nullptr, &plan);
     if (rc) {
       clear_error();
       return 0;  // not eligible: the general path handles it
     }
+    plan->pooled = true;
     if (g_lines_plans.size() >= kLinesPlans) {
       const LinesKey old = g_lines_order.front();
       g_lines_order.erase(g_lines_order.begin());
       lifted_batch_plan* victim = g_lines_plans[old];
       g_lines_plans.erase(old);
-      // a run still in flight keeps using the buffers: wait for it first
-      if (victim->last) cudaEventSynchronize(victim->last);
-      lifted_batch_plan_destroy(victim);
+      lifted_batch_plan_destroy(victim);  // stream-ordered after its last run
     }
     g_lines_plans[{key}] = plan;
     g_lines_order.push_back({key});
@@ -864,11 +879,17 @@ LIFTED_CAPI int lifted_batch_plan_item(const lifted_batch_plan_t* plan, size_t i
 LIFTED_CAPI void lifted_batch_plan_destroy(lifted_batch_plan_t* plan) {
   if (!plan) return;
   if (plan->gexec) cudaGraphExecDestroy(plan->gexec);
+  void* bufs[4] = {plan->d_items, plan->d_progs, plan->d_sync, plan->d_scratch};
+  if (plan->pooled) {
+    // free on the legacy stream after the plan's last run
+    if (plan->last) cudaStreamWaitEvent(nullptr, plan->last, 0);
+    for (void* b : bufs)
+      if (b) cudaFreeAsync(b, nullptr);
+  } else {
+    for (void* b : bufs)
+      if (b) cudaFree(b);
+  }
   if (plan->last) cudaEventDestroy(plan->last);
-  if (plan->d_items) cudaFree(plan->d_items);
-  if (plan->d_progs) cudaFree(plan->d_progs);
-  if (plan->d_sync) cudaFree(plan->d_sync);
-  if (plan->d_scratch) cudaFree(plan->d_scratch);
   cudaGetLastError();
   delete plan;
 }
