@@ -126,6 +126,26 @@ def test_tma_strided_windows_and_whole_lines(op, dtype):
     assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_tma_long_strided_lines(op, dtype):
+    """Long strided lines (windows with halos, the coarse levels on the
+    approximation band in a second launch) with enough line groups for two
+    lines per lane, a 3D view and more levels than the band launch holds in
+    registers: bit for bit against the oracle."""
+    rng = np.random.default_rng(40 + op)
+    cases = [((4096, 2048), [0], [6]), ((2048, 32, 64), [0], [5]), ((4096, 64), [0], [9])]
+    for w in WAVELETS:
+        for shape, axes, lv in cases:
+            x = rng.standard_normal(shape).astype(dtype)
+            rc, o = po.oracle_sep(x, w, op, 0, axes, lv)
+            if rc:
+                continue
+            g, _ = run(x, w, op, 0, axes, lv)
+            assert np.array_equal(g, o), (w, shape, axes, lv)
+    assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
+
+
 def test_rows_two_warps_match_one_warp():
     """float32 rows of 2048 and 4096 split over two warps equal the
     one-warp-per-row kernel (option off) and the oracle."""
