@@ -287,7 +287,12 @@ LIFTED_CAPI uint64_t lifted_launch_count(void);
  *   "long_lines_batched"   0/1  contiguous lines too long for one CTA run
  *                               on the batch engine (many CTAs per line)
  *   "wrow_split"           0/1  float32 rows of 2048/4096 split over two
- *                               warps (else one warp per row) */
+ *                               warps (else one warp per row)
+ *   "overlap_launches"     0/1  programmatic dependent launch: the next
+ *                               transform kernel in a stream is scheduled
+ *                               while the one before it drains, and waits
+ *                               in hardware for its results (launches
+ *                               recorded by stream capture never use it) */
 LIFTED_CAPI int lifted_set_option(const char* name, int64_t value);
 /* Synchronises `stream` and reports LIFTED_ETIMEOUT if a kernel of this
  * library gave up a bounded device-side wait since the last check (the

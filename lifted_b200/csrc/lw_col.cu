@@ -5,6 +5,7 @@
 #include "lw_col.hpp"
 #include "lw_col_kernel.cuh"
 #include "lw_launch.hpp"
+#include "lw_pdl.hpp"
 
 namespace lw {
 namespace {
@@ -23,8 +24,7 @@ cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
-  kern<<<grid, COL_THREADS, smem, stream>>>(p);
-  return cudaGetLastError();
+  return launch_overlapped(kern, grid, COL_THREADS, smem, stream, p);
 }
 
 template <typename T, int WI, int V>

@@ -34,6 +34,7 @@
 
 #include <cstdint>
 
+#include "lw_pdl.hpp"
 #include "lw_reg_kernel.cuh"
 
 namespace lw {
@@ -284,10 +285,12 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
 
   if (tid == 0) col::mbar_init(bar);
   __syncthreads();
+  pdl_wait();  // the previous kernel's results (no global access before)
   uint32_t parity = 0;
   int64_t t = blockIdx.x;
   if (t < p.ntiles && tid == 0) col::issue<T, FWD, V>(p, t, stage, bar);
   for (; t < p.ntiles; t += gridDim.x) {
+    if (t + gridDim.x >= p.ntiles) pdl_trigger();  // the CTA's last tile
     const bool got = col::mbar_wait(bar, parity, p.spin_limit);
     if (!__syncthreads_and(got)) {
       if (tid == 0) atomicExch(p.err, 1);

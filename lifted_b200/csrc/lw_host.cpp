@@ -3,6 +3,8 @@
 // include/lifted_capi.h.
 #include <cuda_runtime.h>
 
+#include "lw_pdl.hpp"
+
 #include <algorithm>
 #include <atomic>
 #include <cfloat>
@@ -73,6 +75,7 @@ std::atomic<int64_t> g_opt_tma_strided{1};
 std::atomic<int64_t> g_opt_tma_packed{1};
 std::atomic<int64_t> g_opt_long_batched{1};
 std::atomic<int64_t> g_opt_wrow_split{1};
+std::atomic<int64_t> g_opt_overlap{1};
 
 }  // namespace
 
@@ -825,6 +828,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_long_batched = value ? 1 : 0;
   } else if (!std::strcmp(name, "wrow_split")) {
     g_opt_wrow_split = value ? 1 : 0;
+  } else if (!std::strcmp(name, "overlap_launches")) {
+    g_opt_overlap = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");
@@ -838,6 +843,7 @@ uint64_t launch_count() { return g_launches.load(); }
 bool col_enabled() { return g_opt_tma_strided.load() != 0; }
 bool col_packed() { return g_opt_tma_packed.load() != 0; }
 bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
+bool pdl_enabled() { return g_opt_overlap.load() != 0; }
 
 }  // namespace lw
 

@@ -12,6 +12,8 @@ namespace {
 // in -> out before working in place, src/lifted-drivers-inl.hpp:542-567).
 template <typename T>
 __global__ void copy_kernel(const __grid_constant__ CopyParams<T> p) {
+  pdl_wait();  // the previous kernel's results (no global access before)
+  pdl_trigger();
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
        li < p.total; li += stride) {
@@ -42,8 +44,7 @@ cudaError_t launch_line_impl(const LineParams<T>& p, int grid, int block,
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
-  line_kernel<T><<<grid, block, smem, stream>>>(p);
-  return cudaGetLastError();
+  return launch_overlapped(line_kernel<T>, grid, block, smem, stream, p);
 }
 
 }  // namespace
@@ -61,15 +62,13 @@ cudaError_t launch_copy(const CopyParams<float>& p, cudaStream_t stream) {
   int grid = (int)((p.total + 255) / 256);
   if (grid > 148 * 16) grid = 148 * 16;
   if (grid < 1) grid = 1;
-  copy_kernel<float><<<grid, 256, 0, stream>>>(p);
-  return cudaGetLastError();
+  return launch_overlapped(copy_kernel<float>, grid, 256, 0, stream, p);
 }
 cudaError_t launch_copy(const CopyParams<double>& p, cudaStream_t stream) {
   int grid = (int)((p.total + 255) / 256);
   if (grid > 148 * 16) grid = 148 * 16;
   if (grid < 1) grid = 1;
-  copy_kernel<double><<<grid, 256, 0, stream>>>(p);
-  return cudaGetLastError();
+  return launch_overlapped(copy_kernel<double>, grid, 256, 0, stream, p);
 }
 
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream) {

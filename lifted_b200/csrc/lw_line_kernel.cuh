@@ -21,6 +21,7 @@
 
 #include <cstdint>
 
+#include "lw_pdl.hpp"
 #include "lw_types.hpp"
 
 namespace lw {
@@ -367,6 +368,8 @@ template <typename T>
 __global__ void __launch_bounds__(512)
     line_kernel(const __grid_constant__ LineParams<T> p) {
   extern __shared__ __align__(16) unsigned char lw_smem_raw[];
+  pdl_wait();  // the previous kernel's results (no global access before)
+  pdl_trigger();
   __shared__ int64_t s_bin[64];
   __shared__ int64_t s_bout[64];
   const LineGeom& g = p.g;

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include "lw_launch.hpp"
+#include "lw_pdl.hpp"
 #include "lw_reg_inst.hpp"
 #include "lw_reg_kernel.cuh"
 
@@ -25,8 +26,7 @@ cudaError_t launch_one(const RegParams<float>& p, int grid, int block,
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
-  kern<<<grid, block, smem, stream>>>(p);
-  return cudaGetLastError();
+  return launch_overlapped(kern, grid, block, smem, stream, p);
 }
 
 template <int WI, int OP>

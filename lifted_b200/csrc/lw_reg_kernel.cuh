@@ -509,6 +509,8 @@ __global__ void __launch_bounds__(512)
   constexpr int HMAX = cat_reach(WI, OP) > 0 ? cat_reach(WI, OP) : 1;
   constexpr bool FWD = (OP == TF_F || OP == TF_IA);
   extern __shared__ __align__(16) unsigned char lw_reg_smem[];
+  pdl_wait();  // the previous kernel's results (no global access before)
+  pdl_trigger();
   reg::Ctx<T> c;
   c.p = &p;
   c.nth = blockDim.x;

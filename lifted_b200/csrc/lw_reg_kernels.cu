@@ -445,6 +445,12 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     int64_t tile, halo, ntr;
     if (n <= COL_ROWS) {
       k = std::min(a.levels, maxreg);
+      // levels past k run on the approximation band: on the whole-line
+      // register kernel when its lines fit one (n <= 32 * p0), else here
+      // again, which needs band lines a multiple of 32 long (float64 lines
+      // of 512 with more levels than the registers hold)
+      if (a.levels > k && n / (2 * p0_of<T>()) > 16)
+        while (k > 0 && ((n >> k) % 32)) --k;
       tile = n;
       halo = 0;
       ntr = 1;
@@ -556,7 +562,12 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       g2.sout = g.nlines;
       for (int d = 0; d < g.nother; ++d) g2.oin[d] = g.oin[d];
       const int r2 = band_pass<T>(a, g2, a.in, tmp, a.levels - k, stream, stats);
-      if (r2 != 1) rc = r2 == 0 ? -2 : r2;
+      if (r2 == 0) {
+        // nothing launched yet: the caller's fallback takes the whole pass
+        scratch_free(tmp, stream);
+        return 0;
+      }
+      if (r2 != 1) rc = r2;
     }
     if (rc == 1) {
       e = fn(cp, grid, smem, stream);

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include "lw_launch.hpp"
+#include "lw_pdl.hpp"
 #include "lw_wrow.hpp"
 #include "lw_wrow2_kernel.cuh"
 
@@ -23,8 +24,7 @@ cudaError_t launch_one(const WRowParams<float>& p, int grid, size_t smem, cudaSt
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
-  kern<<<grid, 128, smem, stream>>>(p);
-  return cudaGetLastError();
+  return launch_overlapped(kern, grid, 128, smem, stream, p);
 }
 
 using Fn = cudaError_t (*)(const WRowParams<float>&, int, size_t, cudaStream_t);

@@ -231,11 +231,13 @@ __global__ void __launch_bounds__(128)
 
   int cur = 0;
   int64_t row = (int64_t)blockIdx.x * 2 + rsel;
+  pdl_wait();  // the previous kernel's results (no global access before)
   if (row < p.g.nlines) load(row, bufs);
   asm volatile("cp.async.commit_group;\n" ::: "memory");
   for (; row < p.g.nlines; row += step) {
     float* buf = bufs + cur * N;
     const int64_t next = row + step;
+    if (next >= p.g.nlines) pdl_trigger();  // the slot's last row
     if (next < p.g.nlines) load(next, bufs + (cur ^ 1) * N);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this row's copy

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include "lw_launch.hpp"
+#include "lw_pdl.hpp"
 #include "lw_wrow.hpp"
 #include "lw_wrow_kernel.cuh"
 
@@ -24,8 +25,7 @@ cudaError_t launch_one(const WRowParams<double>& p, int grid, int block,
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
-  kern<<<grid, block, smem, stream>>>(p);
-  return cudaGetLastError();
+  return launch_overlapped(kern, grid, block, smem, stream, p);
 }
 
 using Fn = cudaError_t (*)(const WRowParams<double>&, int, int, size_t, cudaStream_t);

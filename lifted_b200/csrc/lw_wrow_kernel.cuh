@@ -262,6 +262,8 @@ __global__ void __launch_bounds__(128)
   const int warp = threadIdx.x >> 5;
   const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   if (row >= p.g.nlines) return;  // whole warps only: no block barriers used
+  pdl_wait();  // the previous kernel's results (no global access before)
+  pdl_trigger();
   T* buf = reinterpret_cast<T*>(lw_wrow_smem) + (int64_t)warp * N;
   int64_t bin, bout;
   line_base(p.g, row, bin, bout);

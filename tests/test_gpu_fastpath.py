@@ -146,6 +146,33 @@ def test_tma_long_strided_lines(op, dtype):
     assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
 
 
+def test_overlapped_launches_chain():
+    """Back-to-back calls whose kernels are scheduled early and wait in
+    hardware for the previous kernel (the overlap_launches option): a 2D
+    forward then adjoint chain, later axes in place, equals the same chain
+    with plain launches and the oracle."""
+    rng = np.random.default_rng(28)
+    x = rng.standard_normal((1024, 2048)).astype(np.float32)
+    rc, want = po.oracle_sep(x, 100907, 0, 0, [0, 1], [6, 6])
+    assert rc == 0
+    rc, want2 = po.oracle_sep(want, 100907, 2, 0, [0, 1], [6, 6])
+    assert rc == 0
+    got = []
+    for on in (1, 0):
+        _lib.set_option("overlap_launches", on)
+        try:
+            t = torch.from_numpy(x).cuda()
+            w = torch.empty_like(t)
+            y = torch.empty_like(t)
+            for op, a, b, ax in [(0, t, w, 0), (0, w, w, 1), (2, w, y, 0), (2, y, y, 1)]:
+                pl._lwt(a, 100907, 0, op, (ax,), (6,), 1, out=b)
+            got.append((w.cpu().numpy(), y.cpu().numpy()))
+        finally:
+            _lib.set_option("overlap_launches", 1)
+    for w_, y_ in got:
+        assert np.array_equal(w_, want) and np.array_equal(y_, want2)
+
+
 def test_rows_two_warps_match_one_warp():
     """float32 rows of 2048 and 4096 split over two warps equal the
     one-warp-per-row kernel (option off) and the oracle."""
