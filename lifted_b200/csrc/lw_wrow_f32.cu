@@ -54,10 +54,10 @@ Fn by_wavelet(int wi, int op) {
 
 int wrow_levels_f32(int wi, int op, int p0) {
   switch (p0) {
-    case 8: return (wi == 2 || wi == 4 || wi == 33) ? reg_max_levels(wi, op, 8) : 0;
-    case 16: return (wi == 2 || wi == 4 || wi == 33) ? reg_max_levels(wi, op, 16) : 0;
-    case 32: return (wi == 2 || wi == 4 || wi == 33) ? reg_max_levels(wi, op, 32) : 0;
-    case 64: return (wi == 2 || wi == 4 || wi == 33) ? reg_max_levels(wi, op, 64) : 0;
+    case 8: return (wi == 2 || wi == 4 || wi == 33) ? wrow_max_levels(wi, op, 8) : 0;
+    case 16: return (wi == 2 || wi == 4 || wi == 33) ? wrow_max_levels(wi, op, 16) : 0;
+    case 32: return (wi == 2 || wi == 4 || wi == 33) ? wrow_max_levels(wi, op, 32) : 0;
+    case 64: return (wi == 2 || wi == 4 || wi == 33) ? wrow_max_levels(wi, op, 64) : 0;
     default: return 0;
   }
 }

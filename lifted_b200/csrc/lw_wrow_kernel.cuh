@@ -122,18 +122,19 @@ __device__ __forceinline__ void write_run(T* buf, int e, const T (&v)[PA]) {
   }
 }
 
-// One step over the lane's P pairs; halos by shuffle.
+// One step over the lane's P pairs; halos by shuffle.  Lanes 0 .. last
+// hold the band (last = 31 except on compacted coarse levels).
 template <typename T, int P, int PA, int KIND, int OFF, int NT, int SUB,
           int HL, int HR>
 __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
-                                        const DevStep<T>& st, int lane) {
+                                        const DevStep<T>& st, int lane, int last) {
   static_assert(HL <= P && HR <= P, "step reaches past the neighbour lane");
   T xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
 #pragma unroll
   for (int h = 0; h < HL; ++h) xl[h] = __shfl_up_sync(FULL, x[P - HL + h], 1);
 #pragma unroll
   for (int h = 0; h < HR; ++h) xr[h] = __shfl_down_sync(FULL, x[h], 1);
-  const bool okl = lane > 0, okr = lane < 31;
+  const bool okl = lane > 0, okr = lane < last;
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     T yi = y[i];
@@ -172,7 +173,7 @@ __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
 
 template <typename T, int WI, int OP, int K, int P, int PA>
 __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
-                                       const DevProgram<T>& prog, int lane) {
+                                       const DevProgram<T>& prog, int lane, int last = 31) {
   if constexpr (K < cat_nsteps(WI)) {
     constexpr CStep cs = cstep(WI, OP, K);
     const DevStep<T>& st = prog.st[K];
@@ -184,12 +185,122 @@ __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
         d[i] = d[i] * dm;
       }
     } else if constexpr (cs.y_is_d) {
-      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, lane);
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, lane,
+                                                                            last);
     } else {
-      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, lane);
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, lane,
+                                                                            last);
     }
-    wsteps<T, WI, OP, K + 1, P, PA>(s, d, prog, lane);
+    wsteps<T, WI, OP, K + 1, P, PA>(s, d, prog, lane, last);
   }
+}
+
+// Coarse levels past the register levels (the pairs per lane would drop
+// below the steps' reach): the band is compacted onto fewer lanes through
+// the row buffer, PC pairs per active lane, and every further level halves
+// the active lanes.  Bands this small all use the unswizzled unit layout
+// (run length 1), which is what the banded drain and fill use for them.
+constexpr int pow2_at_least(int r) {
+  int p = 1;
+  while (p < r) p <<= 1;
+  return p;
+}
+template <int WI, int OP>
+constexpr int compact_pairs() {
+  return pow2_at_least(cat_reach(WI, OP) > 1 ? cat_reach(WI, OP) : 1);
+}
+
+// Active lanes take 2*PC consecutive elements (written with run length
+// CHUNK) as PC pairs; the others hold zeros.
+template <typename T, int CHUNK, int PC>
+__device__ __forceinline__ void take_pairs(T* buf, int lane, int act, T (&cs)[PC], T (&cd)[PC]) {
+  T w[2 * PC];
+  if (lane < act) {
+    read_run<T, CHUNK, 2 * PC>(buf, 2 * PC * lane, w);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 2 * PC; ++i) w[i] = T(0);
+  }
+#pragma unroll
+  for (int i = 0; i < PC; ++i) {
+    cs[i] = w[2 * i];
+    cd[i] = w[2 * i + 1];
+  }
+}
+
+// Forward levels lv0 .. levels-1 on a band whose approximation a_lv0 is
+// in s, P elements per lane (32 * P elements).
+template <typename T, int WI, int OP, int P, int PA>
+__device__ __forceinline__ void wcompact_fwd(const T (&s)[PA], T* buf, const DevProgram<T>& prog,
+                                             int levels, int lv0, int lane) {
+  constexpr int PC = compact_pairs<WI, OP>();
+  static_assert(16 * P >= PC, "band too short to compact");
+  write_run<T, P, P>(buf, P * lane, s);
+  __syncwarp();
+  int act = 16 * P / PC;
+  T cs[PC], cd[PC];
+  take_pairs<T, P, PC>(buf, lane, act, cs, cd);
+  __syncwarp();
+  for (int lv = lv0; lv < levels; ++lv) {
+    const int nb = act * PC;  // pairs of this level's band
+    wsteps<T, WI, OP, 0, PC, PC>(cs, cd, prog, lane, act - 1);
+    if (lane < act) write_run<T, 1, PC>(buf, nb + PC * lane, cd);
+    if (lane < act) write_run<T, 1, PC>(buf, PC * lane, cs);
+    if (lv + 1 == levels) return;
+    __syncwarp();
+    act >>= 1;
+    take_pairs<T, 1, PC>(buf, lane, act, cs, cd);
+    __syncwarp();
+  }
+}
+
+// Reverse levels levels-1 .. lv0 (coarsest first); leaves a_lv0 in s, P
+// elements per lane, for the register levels below.
+template <typename T, int WI, int OP, int P, int PA>
+__device__ __forceinline__ void wcompact_rev(T (&s)[PA], T* buf, const DevProgram<T>& prog,
+                                             int levels, int lv0, int lane) {
+  constexpr int PC = compact_pairs<WI, OP>();
+  static_assert(16 * P >= PC, "band too short to compact");
+  int act = ((16 * P) >> (levels - 1 - lv0)) / PC;
+  T cs[PC], cd[PC];
+  if (lane < act) {
+    read_run<T, 1, PC>(buf, PC * lane, cs);  // a_L
+  } else {
+#pragma unroll
+    for (int i = 0; i < PC; ++i) cs[i] = T(0);
+  }
+  for (int lv = levels - 1; lv >= lv0; --lv) {
+    const int nb = act * PC;
+    if (lane < act) {
+      read_run<T, 1, PC>(buf, nb + PC * lane, cd);
+    } else {
+#pragma unroll
+      for (int i = 0; i < PC; ++i) cd[i] = T(0);
+    }
+    wsteps<T, WI, OP, 0, PC, PC>(cs, cd, prog, lane, act - 1);
+    __syncwarp();  // the band is read before a_lv overwrites it
+    if (lane < act) {
+      T w[2 * PC];
+#pragma unroll
+      for (int i = 0; i < PC; ++i) {
+        w[2 * i] = cs[i];
+        w[2 * i + 1] = cd[i];
+      }
+      write_run<T, 1, 2 * PC>(buf, 2 * PC * lane, w);
+    }
+    __syncwarp();
+    if (lv > lv0) {
+      act <<= 1;
+      if (lane < act) {
+        read_run<T, 1, PC>(buf, PC * lane, cs);
+      } else {
+#pragma unroll
+        for (int i = 0; i < PC; ++i) cs[i] = T(0);
+      }
+    }
+  }
+  read_run<T, 1, P>(buf, P * lane, s);
+  __syncwarp();
 }
 
 // Forward-stepping levels: band of level LV+1 has 32*P pairs.
@@ -207,12 +318,16 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
         write_run<T, P, P>(buf, P * lane, s);
         return;
       }
+      if constexpr (LV + 1 >= reg_max_levels(WI, OP, P0)) {
+        wcompact_fwd<T, WI, OP, P, P0>(s, buf, prog, levels, LV + 1, lane);
+      } else {
 #pragma unroll
-      for (int i = 0; i < P / 2; ++i) {
-        d[i] = s[2 * i + 1];
-        s[i] = s[2 * i];
+        for (int i = 0; i < P / 2; ++i) {
+          d[i] = s[2 * i + 1];
+          s[i] = s[2 * i];
+        }
+        wfwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane);
       }
-      wfwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane);
     }
   }
 }
@@ -247,7 +362,18 @@ __device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
 
 // Largest number of levels one warp can run on a row of 64*P0 elements.
 constexpr int wrow_max_levels(int wi, int op, int p0) {
-  return reg_max_levels(wi, op, p0);
+  const int lc = reg_max_levels(wi, op, p0);
+  if (lc < 1) return 0;
+  const int reach = cat_reach(wi, op) > 1 ? cat_reach(wi, op) : 1;
+  int pc = 1;
+  while (pc < reach) pc <<= 1;
+  int act = 16 * (p0 >> (lc - 1)) / pc;  // lanes of the first compacted level
+  int lv = lc;
+  while (act >= 1 && lv < MAX_LEVELS) {
+    ++lv;
+    act >>= 1;
+  }
+  return lv;
 }
 
 template <typename T, int WI, int OP, int P0>
@@ -301,6 +427,8 @@ __global__ void __launch_bounds__(128)
     wrow::wfwd<T, WI, OP, P0, 0>(s, d, buf, p.prog, p.levels, lane);
   } else {
     constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
+    if (p.levels > TOP + 1)
+      wrow::wcompact_rev<T, WI, OP, (P0 >> TOP), P0>(s, buf, p.prog, p.levels, TOP + 1, lane);
     wrow::wrev<T, WI, OP, P0, TOP>(s, d, buf, p.prog, p.levels, lane);
     __syncwarp();
     T x[2 * P0];
