@@ -284,6 +284,9 @@ LIFTED_CAPI uint64_t lifted_launch_count(void);
  *   "fast_path"            0/1  register-blocked kernels where they apply
  *   "tma_strided"          0/1  TMA-staged kernel for strided float32 passes
  *   "tma_packed"           0/1  two adjacent lines per lane in that kernel
+ *   "tma_stacked"          0/1  strided lines of 32..256 samples in a 3D
+ *                               view: one staging window holds 512/n
+ *                               consecutive outer slices
  *   "long_lines_batched"   0/1  contiguous lines too long for one CTA run
  *                               on the batch engine (many CTAs per line)
  *   "wrow_split"           0/1  float32 rows of 2048/4096 split over two

@@ -61,7 +61,8 @@ struct ColParams {
   int32_t rank3;        // tensor maps are 3D
   int32_t a_from_tmp;   // reverse: a_k is in the band buffer (else in `in`)
   int32_t spin_limit;   // mbarrier polls before giving up
-  int32_t pad_;
+  int32_t stack;        // whole lines of 512/stack samples: a tile stacks
+                        // `stack` consecutive outer slices (1: off)
   int32_t* err;         // set to 1 when a staging wait gave up
 };
 
@@ -130,6 +131,7 @@ __device__ __forceinline__ TileCoord decode(const ColParams<T>& p, int64_t t) {
   c.rt = rem - strip * p.ntr;
   c.col0 = strip * COL_LANES * V;
   c.wstart = c.rt * p.r.tile - p.r.halo;
+  c.outer *= p.stack;  // first slice of the tile's group
   return c;
 }
 
@@ -144,8 +146,12 @@ __device__ __forceinline__ void issue(const ColParams<T>& p, int64_t t, T* stage
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   mbar_expect(bar, COL_ROWS * W * sizeof(T));
   if (FWD) {
+    // stacked: slices z .. z+stack-1 of n rows each, two boxes of half the
+    // slices (256 rows each)
+    const bool st = p.stack > 1;
     tma_box(stage, &p.tm_rows[0], x, (int)tc.wstart, z, r3, bar);
-    tma_box(stage + 256 * W, &p.tm_rows[0], x, (int)tc.wstart + 256, z, r3, bar);
+    tma_box(stage + 256 * W, &p.tm_rows[0], x, st ? 0 : (int)tc.wstart + 256,
+            st ? z + p.stack / 2 : z, r3, bar);
   } else {
     // d_l windows at rows m_l + (wstart >> l), l = 1..k, then a_k
     const int k = p.r.nreg;
@@ -156,7 +162,10 @@ __device__ __forceinline__ void issue(const ColParams<T>& p, int64_t t, T* stage
               r3, bar);
       row += COL_ROWS >> l;
     }
-    if (p.a_from_tmp) {
+    if (p.a_from_tmp && p.stack > 1) {
+      // band buffer viewed as {lines of a slice, position, slice}
+      tma_box(stage + (size_t)row * W, &p.tm_tmp, x, 0, z, true, bar);
+    } else if (p.a_from_tmp) {
       // band buffer: x = line index, y = position
       const int64_t L0 = tc.outer * p.ncols + tc.col0;
       tma_box(stage + (size_t)row * W, &p.tm_tmp, (int)L0, (int)(tc.wstart >> k), 0, false, bar);
@@ -282,6 +291,11 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   c.has_l = c.r > 0;
   c.has_r = c.r < COL_CHUNKS - 1;
   c.n = p.r.g.n;
+  // stacked tiles: chunk r holds chunk rr of slice zr (its own line, whose
+  // band edges mask the taps that would reach the neighbouring slices)
+  const int cps = p.stack > 1 ? (int)(c.n / (2 * P0)) : COL_CHUNKS;
+  const int zr = c.r / cps;
+  const int rr = c.r - zr * cps;
 
   if (tid == 0) col::mbar_init(bar);
   __syncthreads();
@@ -299,14 +313,17 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
     }
     parity ^= 1;
     const col::TileCoord tc = col::decode<T, V>(p, t);
-    const int64_t L = tc.outer * p.ncols + tc.col0 + (int64_t)c.j * V;
+    const int64_t outer = tc.outer + zr;
+    const int64_t L = outer * p.ncols + tc.col0 + (int64_t)c.j * V;
     c.L = L;
-    c.line_ok = L < p.r.g.nlines;  // V lines together (ncols % (32 V) == 0)
+    // V lines together (ncols % (32 V) == 0); a last group of stacked
+    // slices may run past the outer extent
+    c.line_ok = outer < p.nouter && L < p.r.g.nlines;
     c.bin = 0;
     c.bout = 0;
     if (c.line_ok) line_base(p.r.g, L, c.bin, c.bout);
     c.buf = 0;
-    c.e0 = tc.wstart + (int64_t)2 * P0 * c.r;
+    c.e0 = tc.wstart + (int64_t)2 * P0 * rr;
     c.tile_lo = tc.rt * p.r.tile;
     c.tile_hi = c.tile_lo + p.r.tile < c.n ? c.tile_lo + p.r.tile : c.n;
     const int64_t next = t + gridDim.x;

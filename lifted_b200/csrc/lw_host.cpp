@@ -73,6 +73,7 @@ std::atomic<int64_t> g_opt_max_global_ctas{296};
 std::atomic<int64_t> g_opt_fast_path{1};
 std::atomic<int64_t> g_opt_tma_strided{1};
 std::atomic<int64_t> g_opt_tma_packed{1};
+std::atomic<int64_t> g_opt_tma_stacked{1};
 std::atomic<int64_t> g_opt_long_batched{1};
 std::atomic<int64_t> g_opt_wrow_split{1};
 std::atomic<int64_t> g_opt_overlap{1};
@@ -824,6 +825,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_tma_strided = value ? 1 : 0;
   } else if (!std::strcmp(name, "tma_packed")) {
     g_opt_tma_packed = value ? 1 : 0;
+  } else if (!std::strcmp(name, "tma_stacked")) {
+    g_opt_tma_stacked = value ? 1 : 0;
   } else if (!std::strcmp(name, "long_lines_batched")) {
     g_opt_long_batched = value ? 1 : 0;
   } else if (!std::strcmp(name, "wrow_split")) {
@@ -842,6 +845,7 @@ int set_option(const char* name, int64_t value) {
 uint64_t launch_count() { return g_launches.load(); }
 bool col_enabled() { return g_opt_tma_strided.load() != 0; }
 bool col_packed() { return g_opt_tma_packed.load() != 0; }
+bool col_stacked() { return g_opt_tma_stacked.load() != 0; }
 bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
 bool pdl_enabled() { return g_opt_overlap.load() != 0; }
 

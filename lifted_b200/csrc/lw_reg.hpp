@@ -35,6 +35,9 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats)
 bool col_enabled();
 // Whether it may pack two adjacent lines per lane (the "tma_packed" option).
 bool col_packed();
+// Whether short strided lines of a 3D view stack several outer slices in
+// one staging window (the "tma_stacked" option).
+bool col_stacked();
 // Synchronises `stream`; returns 1 (and clears it) if a TMA-staged kernel
 // gave up waiting for a staging copy since the last check, 0 if not, -1 if
 // the check itself failed.

@@ -400,10 +400,10 @@ EncodeTiledFn encode_tiled_fn() {
 
 bool encode_rows(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims,
                  const cuuint64_t* strides, cuuint32_t box_x, cuuint32_t box_y,
-                 int elem_bytes) {
+                 int elem_bytes, cuuint32_t box_z = 1) {
   EncodeTiledFn enc = encode_tiled_fn();
   if (!enc) return false;
-  const cuuint32_t box[3] = {box_x, box_y, 1};
+  const cuuint32_t box[3] = {box_x, box_y, box_z};
   const cuuint32_t es[3] = {1, 1, 1};
   return enc(m, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
              (cuuint32_t)rank, const_cast<void*>(base),
@@ -470,8 +470,15 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       ntr = (n + tile - 1) / tile;
     }
     if (k < 1) return 0;
+    const int64_t nouter = g.nother == 2 ? g.oshape[1] : 1;
+    // short whole lines of a 3D view: a tile stacks 512/n consecutive outer
+    // slices (the staging window stays full)
+    int stack = 1;
+    if (col_stacked() && n <= COL_ROWS / 2 && COL_ROWS % n == 0 && g.nother == 2 && nouter >= 2)
+      stack = (int)(COL_ROWS / n);
+    const int64_t ngroups = (nouter + stack - 1) / stack;
     // packed lanes only while they still give every SM a tile
-    if (v == 2 && ncols / (2 * COL_LANES) * ntr * (g.nother == 2 ? g.oshape[1] : 1) < sm_count())
+    if (v == 2 && ncols / (2 * COL_LANES) * ntr * ngroups < sm_count())
       v = 1;
     ColFn<T> fn;
     if constexpr (sizeof(T) == 4) fn = pick_col_f32(wi, op, v);
@@ -498,9 +505,31 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
                                    (cuuint64_t)(g.nother == 2 ? g.oin[1] : 0) * EB};
     bool ok = true;
     const cuuint32_t bx = (cuuint32_t)(COL_LANES * v);
-    for (int i = 0; i < k && ok; ++i)
-      ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, bx, (cuuint32_t)(256 >> i), EB);
-    if (ok && more) {
+    const bool fwd_op = (op == TF_F || op == TF_IA);
+    if (stack > 1) {
+      // forward: two boxes of stack/2 slices x n rows; reverse: region l of
+      // every slice (n >> l rows) in one box of all the slices
+      if (fwd_op) {
+        ok = encode_rows(&cp.tm_rows[0], a.in, rank, dims, strides, bx, (cuuint32_t)n, EB,
+                         (cuuint32_t)(stack / 2));
+      } else {
+        for (int i = 0; i < k && ok; ++i)
+          ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, bx,
+                           (cuuint32_t)(n >> (i + 1)), EB, (cuuint32_t)stack);
+      }
+    } else {
+      for (int i = 0; i < k && ok; ++i)
+        ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, bx, (cuuint32_t)(256 >> i),
+                         EB);
+    }
+    if (ok && more && stack > 1) {
+      // the band buffer [position][line] viewed as {line in slice, position,
+      // slice}
+      const cuuint64_t tdims[3] = {(cuuint64_t)ncols, (cuuint64_t)m, (cuuint64_t)nouter};
+      const cuuint64_t tstr[2] = {(cuuint64_t)g.nlines * EB, (cuuint64_t)ncols * EB};
+      ok = encode_rows(&cp.tm_tmp, tmp, 3, tdims, tstr, bx, (cuuint32_t)m, EB,
+                       (cuuint32_t)stack);
+    } else if (ok && more) {
       const cuuint64_t tdims[2] = {(cuuint64_t)g.nlines, (cuuint64_t)m};
       const cuuint64_t tstr[1] = {(cuuint64_t)g.nlines * EB};
       ok = encode_rows(&cp.tm_tmp, tmp, 2, tdims, tstr, bx, (cuuint32_t)(COL_ROWS >> k), EB);
@@ -525,9 +554,10 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     r.ntiles = ntr;
     r.prog = *a.prog;
     cp.ncols = ncols;
-    cp.nouter = g.nother == 2 ? g.oshape[1] : 1;
+    cp.nouter = nouter;
     cp.ntr = ntr;
-    cp.ntiles = ncols / (COL_LANES * v) * ntr * cp.nouter;
+    cp.ntiles = ncols / (COL_LANES * v) * ntr * ngroups;
+    cp.stack = stack;
     cp.rank3 = rank == 3;
     cp.a_from_tmp = more ? 1 : 0;
     cp.spin_limit = 1 << 22;

@@ -146,6 +146,34 @@ def test_tma_long_strided_lines(op, dtype):
     assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_tma_stacked_short_lines(op, dtype):
+    """Strided lines of 32 .. 256 samples in 3D views, several outer slices
+    per staging window (outer extents that leave a last, partial group),
+    and a 512-sample axis whose coarse band launch stacks: bit for bit
+    against the oracle and against unstacked windows."""
+    rng = np.random.default_rng(50 + op)
+    cases = [((64, 40, 64), [0], [2]), ((32, 7, 96), [0], [1]), ((128, 3, 64), [0], [3]),
+             ((256, 5, 128), [0], [4]), ((9, 64, 32), [1], [3]), ((512, 24, 64), [0], [4]),
+             ((64, 64, 64), [0, 1, 2], [3, 3, 3])]
+    for w in WAVELETS:
+        for shape, axes, lv in cases:
+            x = rng.standard_normal(shape).astype(dtype)
+            rc, o = po.oracle_sep(x, w, op, 0, axes, lv)
+            if rc:
+                continue
+            g, _ = run(x, w, op, 0, axes, lv)
+            assert np.array_equal(g, o), (w, shape, axes, lv)
+            _lib.set_option("tma_stacked", 0)
+            try:
+                g2, _ = run(x, w, op, 0, axes, lv)
+            finally:
+                _lib.set_option("tma_stacked", 1)
+            assert np.array_equal(g2, o), (w, shape, axes, lv)
+    assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
+
+
 def test_overlapped_launches_chain():
     """Back-to-back calls whose kernels are scheduled early and wait in
     hardware for the previous kernel (the overlap_launches option): a 2D
