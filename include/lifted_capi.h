@@ -291,6 +291,9 @@ LIFTED_CAPI uint64_t lifted_launch_count(void);
  *                               on the batch engine (many CTAs per line)
  *   "wrow_split"           0/1  float32 rows of 2048/4096 split over two
  *                               warps (else one warp per row)
+ *   "row_windows"          0/1  contiguous rows longer than one warp holds
+ *                               run every level on windows with halos,
+ *                               one warp each (else the batch engine)
  *   "overlap_launches"     0/1  programmatic dependent launch: the next
  *                               transform kernel in a stream is scheduled
  *                               while the one before it drains, and waits

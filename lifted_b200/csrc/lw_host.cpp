@@ -77,6 +77,7 @@ std::atomic<int64_t> g_opt_tma_stacked{1};
 std::atomic<int64_t> g_opt_long_batched{1};
 std::atomic<int64_t> g_opt_wrow_split{1};
 std::atomic<int64_t> g_opt_overlap{1};
+std::atomic<int64_t> g_opt_row_windows{1};
 
 }  // namespace
 
@@ -833,6 +834,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_wrow_split = value ? 1 : 0;
   } else if (!std::strcmp(name, "overlap_launches")) {
     g_opt_overlap = value ? 1 : 0;
+  } else if (!std::strcmp(name, "row_windows")) {
+    g_opt_row_windows = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");
@@ -848,6 +851,7 @@ bool col_packed() { return g_opt_tma_packed.load() != 0; }
 bool col_stacked() { return g_opt_tma_stacked.load() != 0; }
 bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
 bool pdl_enabled() { return g_opt_overlap.load() != 0; }
+bool wtile_enabled() { return g_opt_row_windows.load() != 0; }
 
 }  // namespace lw
 

@@ -15,6 +15,7 @@
 #include "lw_launch.hpp"
 #include "lw_reg.hpp"
 #include "lw_reg_inst.hpp"
+#include "lw_wtile_kernel.cuh"
 #include "lw_reg_kernel.cuh"
 #include "lw_wrow.hpp"
 #include "lw_wrow_kernel.cuh"
@@ -229,6 +230,47 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     e = launch_wrow_f32(a.wi, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
   else
     e = launch_wrow_f64(a.wi, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
+  if (e != cudaSuccess) return -(int)e - 1000;
+  if (stats) stats->launches += 1;
+  return 1;
+}
+
+// Contiguous rows longer than one warp holds: every level on windows of
+// 64 * P0 samples with halos (lw_wtile_kernel.cuh), one launch.
+template <typename T>
+int launch_wtile(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
+  const LineGeom& g = a.g;
+  if (!wtile_enabled() || a.in_place) return 0;  // windows read other windows' input
+  if (!rows_vectorisable(g, a.in, a.out)) return 0;
+  const int p0 = wtile_pairs((int)sizeof(T));
+  const int64_t W = 64 * (int64_t)p0;
+  const int64_t n = g.n;
+  if (n <= W || n % (2 * p0)) return 0;
+  if (a.levels < 1 || a.levels > wtile_levels(a.wi, a.op, (int)sizeof(T))) return 0;
+  // halo: the samples k levels corrupt from a window edge, whole lanes
+  int64_t need = 0;
+  const int lh = cat_level_halo(a.wi, a.op);
+  for (int l = 1; l <= a.levels; ++l) need += (int64_t)lh << l;
+  const int64_t halo = (need + 2 * p0 - 1) / (2 * p0) * (2 * p0);
+  const int64_t tile = W - 2 * halo;
+  if (tile < W / 4) return 0;
+  WTileParams<T> p;
+  std::memset(&p, 0, sizeof(p));
+  p.in = a.in;
+  p.out = a.out;
+  p.g = g;
+  p.tile = tile;
+  p.halo = halo;
+  p.ntiles = (n + tile - 1) / tile;
+  p.levels = a.levels;
+  p.prog = *a.prog;
+  const int warps = 4;
+  const int64_t grid = (g.nlines * p.ntiles + warps - 1) / warps;
+  if (grid > 0x7fffffffLL) return 0;
+  const size_t smem = (size_t)warps * (size_t)W * sizeof(T);
+  cudaError_t e;
+  if constexpr (sizeof(T) == 4) e = launch_wtile_f32(a.wi, a.op, p, (int)grid, smem, stream);
+  else e = launch_wtile_f64(a.wi, a.op, p, (int)grid, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
   if (stats) stats->launches += 1;
   return 1;
@@ -663,6 +705,8 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
   // whole lines: contiguous rows, or strided lines adjacent in memory
   if (contiguous) {
     int rc = launch_wrow<T>(a, stream, stats);
+    if (rc != 0) return rc;
+    rc = launch_wtile<T>(a, stream, stats);
     if (rc != 0) return rc;
     rc = launch_whole<T>(a, g, a.in, a.out, a.levels, false, stream, stats);
     if (rc != 0) return rc;

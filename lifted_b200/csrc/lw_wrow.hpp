@@ -31,4 +31,18 @@ int wrow2_resident_ctas(int p0);
 // Whether contiguous float32 rows may use it (the "wrow_split" option).
 bool wrow2_enabled();
 
+// Windowed rows (rows longer than one warp holds): pairs per lane of the
+// window (32 for float32, 16 for float64), levels compiled for (catalogue
+// wavelet, transform), launchers.
+template <typename T>
+struct WTileParams;
+int wtile_pairs(int elem_bytes);
+int wtile_levels(int wi, int op, int elem_bytes);
+cudaError_t launch_wtile_f32(int wi, int op, const WTileParams<float>& p, int grid, size_t smem,
+                             cudaStream_t stream);
+cudaError_t launch_wtile_f64(int wi, int op, const WTileParams<double>& p, int grid, size_t smem,
+                             cudaStream_t stream);
+// Whether long contiguous rows may use it (the "row_windows" option).
+bool wtile_enabled();
+
 }  // namespace lw

@@ -122,19 +122,19 @@ __device__ __forceinline__ void write_run(T* buf, int e, const T (&v)[PA]) {
   }
 }
 
-// One step over the lane's P pairs; halos by shuffle.  Lanes 0 .. last
-// hold the band (last = 31 except on compacted coarse levels).
+// One step over the lane's P pairs; halos by shuffle.  okl / okr: the
+// left / right neighbour lane holds pairs of the same band (whole rows:
+// lane > 0 / lane < the last active lane; windows: also by band position).
 template <typename T, int P, int PA, int KIND, int OFF, int NT, int SUB,
           int HL, int HR>
 __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
-                                        const DevStep<T>& st, int lane, int last) {
+                                        const DevStep<T>& st, bool okl, bool okr) {
   static_assert(HL <= P && HR <= P, "step reaches past the neighbour lane");
   T xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
 #pragma unroll
   for (int h = 0; h < HL; ++h) xl[h] = __shfl_up_sync(FULL, x[P - HL + h], 1);
 #pragma unroll
   for (int h = 0; h < HR; ++h) xr[h] = __shfl_down_sync(FULL, x[h], 1);
-  const bool okl = lane > 0, okr = lane < last;
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     T yi = y[i];
@@ -173,7 +173,7 @@ __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
 
 template <typename T, int WI, int OP, int K, int P, int PA>
 __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
-                                       const DevProgram<T>& prog, int lane, int last = 31) {
+                                       const DevProgram<T>& prog, bool okl, bool okr) {
   if constexpr (K < cat_nsteps(WI)) {
     constexpr CStep cs = cstep(WI, OP, K);
     const DevStep<T>& st = prog.st[K];
@@ -185,13 +185,13 @@ __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
         d[i] = d[i] * dm;
       }
     } else if constexpr (cs.y_is_d) {
-      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, lane,
-                                                                            last);
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, okl,
+                                                                            okr);
     } else {
-      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, lane,
-                                                                            last);
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, okl,
+                                                                            okr);
     }
-    wsteps<T, WI, OP, K + 1, P, PA>(s, d, prog, lane, last);
+    wsteps<T, WI, OP, K + 1, P, PA>(s, d, prog, okl, okr);
   }
 }
 
@@ -243,7 +243,7 @@ __device__ __forceinline__ void wcompact_fwd(const T (&s)[PA], T* buf, const Dev
   __syncwarp();
   for (int lv = lv0; lv < levels; ++lv) {
     const int nb = act * PC;  // pairs of this level's band
-    wsteps<T, WI, OP, 0, PC, PC>(cs, cd, prog, lane, act - 1);
+    wsteps<T, WI, OP, 0, PC, PC>(cs, cd, prog, lane > 0, lane < act - 1);
     if (lane < act) write_run<T, 1, PC>(buf, nb + PC * lane, cd);
     if (lane < act) write_run<T, 1, PC>(buf, PC * lane, cs);
     if (lv + 1 == levels) return;
@@ -277,7 +277,7 @@ __device__ __forceinline__ void wcompact_rev(T (&s)[PA], T* buf, const DevProgra
 #pragma unroll
       for (int i = 0; i < PC; ++i) cd[i] = T(0);
     }
-    wsteps<T, WI, OP, 0, PC, PC>(cs, cd, prog, lane, act - 1);
+    wsteps<T, WI, OP, 0, PC, PC>(cs, cd, prog, lane > 0, lane < act - 1);
     __syncwarp();  // the band is read before a_lv overwrites it
     if (lane < act) {
       T w[2 * PC];
@@ -312,7 +312,7 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
   if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
     if (LV < levels) {
       constexpr int NB = 32 * P;  // band length at this level
-      wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane);
+      wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane > 0, lane < 31);
       write_run<T, P, P>(buf, NB + P * lane, d);
       if (LV + 1 == levels) {
         write_run<T, P, P>(buf, P * lane, s);
@@ -344,7 +344,7 @@ __device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
         constexpr int NB = 32 * P;
         if (LV + 1 == levels) read_run<T, P, P>(buf, P * lane, s);
         read_run<T, P, P>(buf, NB + P * lane, d);
-        wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane);
+        wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane > 0, lane < 31);
         if constexpr (LV > 0) {
 #pragma unroll
           for (int i = P - 1; i >= 0; --i) {

@@ -174,6 +174,32 @@ def test_tma_stacked_short_lines(op, dtype):
     assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_long_rows_on_windows(op, dtype):
+    """Contiguous rows longer than one warp holds, every level on windows
+    with halos (first and last windows clipped by the row, a last window
+    shorter than the others): bit for bit against the oracle and against
+    the batch engine that serves them with the option off."""
+    rng = np.random.default_rng(60 + op)
+    cases = [((3, 65536), [2, 5]), ((2, 8192), [1, 4, 6]), ((4, 6080), [3]), ((1, 2112), [2, 5])]
+    for w in WAVELETS:
+        for shape, lvs in cases:
+            for lv in lvs:
+                x = rng.standard_normal(shape).astype(dtype)
+                rc, o = po.oracle_sep(x, w, op, 0, [1], [lv])
+                if rc:
+                    continue
+                g, _ = run(x, w, op, 0, [1], [lv])
+                assert np.array_equal(g, o), (w, shape, lv)
+                _lib.set_option("row_windows", 0)
+                try:
+                    g2, _ = run(x, w, op, 0, [1], [lv])
+                finally:
+                    _lib.set_option("row_windows", 1)
+                assert np.array_equal(g2, o), (w, shape, lv)
+
+
 def test_overlapped_launches_chain():
     """Back-to-back calls whose kernels are scheduled early and wait in
     hardware for the previous kernel (the overlap_launches option): a 2D
