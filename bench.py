@@ -366,8 +366,9 @@ def inverse_section(dev, x, steps: int = 10):
 def cfg1_section(dev, steps: int = 10):
     """Plain 1D float64: 64 signals of 65536 i.i.d. N(0,1) (seed 1001),
     Daubechies2, 5 levels along axis 1, Zero boundary, Forward then
-    ForwardAdjoint (the long lines run on the batch engine, many CTAs per
-    line), timed as a CUDA graph replay; plus the dot-product test
+    ForwardAdjoint (the long rows run on the windowed row kernel, one warp
+    per window of 1024 samples), timed as a CUDA graph replay; plus the
+    dot-product test
     <W x, r> = <x, W^T r>."""
     import torch
     from lifted_b200 import pylifted as pl
@@ -553,6 +554,9 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched, autograd and least-squares sections")
+    ap.add_argument("--section", choices=["inverse", "cfg1", "batched", "autograd", "lsq"],
+                    help="run only this section (one GPU) and print its JSON; for profiling "
+                         "its kernels, not a driver line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -568,6 +572,17 @@ def main() -> int:
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    if args.section:
+        sys.path.insert(0, str(ROOT))
+        if args.section == "inverse":
+            xi = torch.from_numpy(make_image(SEED)).to(dev)
+            res = inverse_section(dev, xi)
+        else:
+            fn = {"cfg1": cfg1_section, "batched": batched_section,
+                  "autograd": autograd_section, "lsq": lsq_section}[args.section]
+            res = fn(dev)
+        print(json.dumps({"section": args.section, **res}))
+        return 0
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
