@@ -305,6 +305,15 @@ LIFTED_CAPI int lifted_set_option(const char* name, int64_t value);
  * affected output is not valid).  Clears the condition. */
 LIFTED_CAPI int lifted_device_check(void* stream);
 
+/* Blur operator of the wavelet-regularised least-squares form (no
+ * counterpart in the reference, which has no solver): 2D correlation of each
+ * of `nimg` contiguous h x w float32 images with a k x k kernel (odd k <= 7,
+ * row-major host array), zero padding, same size; adjoint != 0 correlates
+ * with the flipped kernel (the transpose).  Device pointers, no overlap,
+ * stream-ordered. */
+LIFTED_CAPI int lifted_blur2d_f32(const float* in, float* out, size_t nimg, size_t h, size_t w,
+                                  const float* kernel, size_t k, int adjoint, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,6 +118,7 @@ _SIGS["lifted_last_error"] = (ctypes.c_char_p, [])
 _SIGS["lifted_launch_count"] = (ctypes.c_uint64, [])
 _SIGS["lifted_set_option"] = (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64])
 _SIGS["lifted_device_check"] = (ctypes.c_int, [_p])
+_SIGS["lifted_blur2d_f32"] = (ctypes.c_int, [_p, _p, _sz, _sz, _sz, _p, _sz, ctypes.c_int, _p])
 
 # Exported names the header declares (checked by the CPU test suite).
 EXPORTED = tuple(_SIGS)

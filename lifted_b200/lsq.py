@@ -12,11 +12,18 @@ adjoint kernel, not from saved activations.
 ground truth of random rectangles, b = A x_true + noise); ``GradientLoop``
 runs the steps on the GPU; the float64 CPU check of the same iteration lives
 in the tests (it uses the oracle).
+
+A is applied by the library's own float32 correlation kernel
+(``lifted_blur2d_f32``), forward and adjoint, so the gradient of the data
+term carries no TF32 rounding.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
+from . import _lib
 from . import autograd as ag
 
 
@@ -62,6 +69,44 @@ def blur_adj_np(y: np.ndarray, k: np.ndarray) -> np.ndarray:
     return blur_np(y, k[::-1, ::-1])
 
 
+def blur2d(x, kernel: np.ndarray, adjoint: bool = False):
+    """A x (or A^T x) for a float32 CUDA tensor (..., h, w): correlation of
+    each image with `kernel` (odd size <= 7), zero padding, same size."""
+    import torch
+
+    if x.dtype != torch.float32 or not x.is_cuda:
+        raise TypeError("blur2d takes a float32 CUDA tensor")
+    x = x.contiguous()
+    out = torch.empty_like(x)
+    k = np.ascontiguousarray(kernel, dtype=np.float32)
+    h, w = x.shape[-2], x.shape[-1]
+    nimg = x.numel() // max(h * w, 1)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    _lib.check(lib.lifted_blur2d_f32(x.data_ptr(), out.data_ptr(), nimg, h, w,
+                                     k.ctypes.data_as(ctypes.c_void_p), k.shape[0],
+                                     1 if adjoint else 0, stream))
+    return out
+
+
+def _blur_function():
+    import torch
+
+    class Blur(torch.autograd.Function):
+        """A as an autograd Function: backward is A^T (the flipped kernel)."""
+
+        @staticmethod
+        def forward(ctx, x, kernel):
+            ctx.kernel = kernel
+            return blur2d(x, kernel)
+
+        @staticmethod
+        def backward(ctx, g):
+            return blur2d(g, ctx.kernel, adjoint=True), None
+
+    return Blur
+
+
 class GradientLoop:
     """Gradient descent on the loss above, float32 on one CUDA device."""
 
@@ -71,19 +116,15 @@ class GradientLoop:
 
         self.torch = torch
         self.b = torch.as_tensor(b, dtype=torch.float32, device=device)
-        k = torch.as_tensor(np.ascontiguousarray(kernel), dtype=torch.float32, device=device)
-        self.k = k[None, None]
+        self.kernel = np.ascontiguousarray(kernel, dtype=np.float32)
+        self._blur = _blur_function()
         self.lam, self.step_size = float(lam), float(step)
         nd = self.b.ndim
         self.W = ag.DWT(wavelet, "Zero", axes=(nd - 2, nd - 1), level=tuple(levels))
         self.x = torch.zeros_like(self.b, requires_grad=True)
 
     def blur(self, x):
-        torch = self.torch
-        shp = x.shape
-        y = torch.nn.functional.conv2d(x.reshape(-1, 1, shp[-2], shp[-1]), self.k,
-                                       padding=self.k.shape[-1] // 2)
-        return y.reshape(shp)
+        return self._blur.apply(x, self.kernel)
 
     def loss(self, x):
         r = self.blur(x) - self.b

@@ -49,3 +49,36 @@ def test_blur_adjoint_is_transpose():
     lhs = np.sum(lsq.blur_np(x, k) * y)
     rhs = np.sum(x * lsq.blur_adj_np(y, k))
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+@pytest.mark.parametrize("ksize", [3, 5, 7])
+def test_blur_kernel_matches_float64(ksize):
+    """The library's blur (A and A^T) against the float64 numpy reference:
+    float32 accumulation of at most 49 products, tolerance 1e-6 of the
+    image scale; sizes that leave partial tiles."""
+    rng = np.random.default_rng(11 + ksize)
+    k = rng.uniform(0.1, 1.0, (ksize, ksize))
+    k /= k.sum()
+    for shape in [(3, 100, 77), (1, 2048, 64), (2, 33, 130)]:
+        x = rng.standard_normal(shape).astype(np.float32)
+        xt = torch.from_numpy(x).cuda()
+        for adj, ref in ((False, lsq.blur_np), (True, lsq.blur_adj_np)):
+            got = lsq.blur2d(xt, k, adjoint=adj).cpu().numpy()
+            want = ref(x.astype(np.float64), k.astype(np.float32).astype(np.float64))
+            assert np.max(np.abs(got - want)) <= 1e-6 * np.max(np.abs(want)) * ksize, (shape, adj)
+
+
+def test_blur_abi_checks():
+    import ctypes
+    from lifted_b200 import _lib
+
+    lib = _lib.load()
+    x = torch.zeros(1, 16, 16, device="cuda")
+    y = torch.zeros_like(x)
+    k = np.ones((4, 4), dtype=np.float32)
+    s = torch.cuda.current_stream().cuda_stream
+    kp = k.ctypes.data_as(ctypes.c_void_p)
+    assert lib.lifted_blur2d_f32(x.data_ptr(), y.data_ptr(), 1, 16, 16, kp, 4, 0, s) == _lib.EINVAL
+    h = np.zeros(256, dtype=np.float32)
+    assert lib.lifted_blur2d_f32(h.ctypes.data, y.data_ptr(), 1, 16, 16, kp, 3, 0, s) == _lib.EINVAL
+    assert lib.lifted_blur2d_f32(x.data_ptr(), x.data_ptr(), 1, 16, 16, kp, 3, 0, s) == _lib.EINVAL
