@@ -186,6 +186,34 @@ typedef struct lifted_signal {
   uint64_t out_offset;  /* element offset of its result in `out` */
 } lifted_signal_t;
 
+/* Batched nD images (no single counterpart in the reference: a loop of
+ * lifted::lwt calls, src/lifted.hpp:13-39, one per image).  Each image is a
+ * dense C-order array of ndim (1..4) axes, transformed separably over all of
+ * them, in order, exactly as
+ *     lifted_lwt_sep_xxx(wavelet, op, bc, ndim, shape, dense strides, ndim,
+ *                        {0, .., ndim-1}, levels, in + in_offset,
+ *                        out + out_offset, stream)
+ * would.  Consecutive entries with the same wavelet, shape and levels whose
+ * data lie back to back in both buffers run as one call over a (group,
+ * shape...) view.  Device pointers; outputs must be disjoint and no image's
+ * output may overlap another image's input (an image may be in place).
+ * Stream-ordered, no synchronisation; on an error, the groups before the
+ * failing one have been enqueued. */
+typedef struct lifted_image {
+  uint32_t wavelet;     /* lifted::Wavelet value */
+  uint32_t ndim;        /* 1..4 */
+  uint64_t shape[4];    /* C order, slowest axis first; entries >= ndim unused */
+  uint32_t levels[4];   /* levels per axis; 0 = max_level(width, length) */
+  uint64_t in_offset;   /* element offset of the image in `in` */
+  uint64_t out_offset;  /* element offset of its result in `out` */
+} lifted_image_t;
+LIFTED_CAPI int lifted_lwt_batch_nd_f32(uint32_t op, uint32_t bc, size_t nimages,
+                                        const lifted_image_t* images, const float* in,
+                                        float* out, void* stream);
+LIFTED_CAPI int lifted_lwt_batch_nd_f64(uint32_t op, uint32_t bc, size_t nimages,
+                                        const lifted_image_t* images, const double* in,
+                                        double* out, void* stream);
+
 /* Optional planner settings (0 = default or autotuned):
  *   block        threads per CTA of the persistent kernel (64..512)
  *   whole_max    longest band transformed as one whole item in shared

@@ -61,6 +61,19 @@ class Signal(ctypes.Structure):
     ]
 
 
+class Image(ctypes.Structure):
+    """lifted_image_t."""
+
+    _fields_ = [
+        ("wavelet", ctypes.c_uint32),
+        ("ndim", ctypes.c_uint32),
+        ("shape", ctypes.c_uint64 * 4),
+        ("levels", ctypes.c_uint32 * 4),
+        ("in_offset", ctypes.c_uint64),
+        ("out_offset", ctypes.c_uint64),
+    ]
+
+
 class BatchTuning(ctypes.Structure):
     """lifted_batch_tuning_t."""
 
@@ -118,6 +131,8 @@ _SIGS["lifted_last_error"] = (ctypes.c_char_p, [])
 _SIGS["lifted_launch_count"] = (ctypes.c_uint64, [])
 _SIGS["lifted_set_option"] = (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64])
 _SIGS["lifted_device_check"] = (ctypes.c_int, [_p])
+_SIGS["lifted_lwt_batch_nd_f32"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
+_SIGS["lifted_lwt_batch_nd_f64"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
 _SIGS["lifted_blur2d_f32"] = (ctypes.c_int, [_p, _p, _sz, _sz, _sz, _p, _sz, ctypes.c_int, _p])
 
 # Exported names the header declares (checked by the CPU test suite).

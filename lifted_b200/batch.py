@@ -179,6 +179,73 @@ def lwt_batch(x, lengths, wavelets, levels=0, op=Transform.Forward, mode="Zero",
         plan.close()
 
 
+def image_table(shapes, wavelets, levels=0, in_offsets=None, out_offsets=None):
+    """lifted_image_t array for images of the given shapes (C order, 1..4
+    axes).  ``levels``: one int for every axis of every image, or one entry
+    per image (an int or a per-axis sequence).  Offsets default to the
+    packed layout (images back to back, the same offsets in and out)."""
+    n = len(shapes)
+    if isinstance(wavelets, (str, int)) or not hasattr(wavelets, "__len__"):
+        wavelets = [wavelets] * n
+    if isinstance(levels, (int, np.integer)):
+        levels = [int(levels)] * n
+    if len(wavelets) != n or len(levels) != n:
+        raise ValueError("shapes, wavelets and levels differ in length")
+    sizes = [int(np.prod(s)) for s in shapes]
+    packed = np.concatenate([[0], np.cumsum(sizes)[:-1]]) if n else np.zeros(0, np.int64)
+    ino = packed if in_offsets is None else np.asarray(in_offsets, dtype=np.int64)
+    outo = ino if out_offsets is None else np.asarray(out_offsets, dtype=np.int64)
+    tab = (_lib.Image * max(n, 1))()
+    for i, shp in enumerate(shapes):
+        shp = tuple(int(v) for v in shp)
+        if not 1 <= len(shp) <= 4:
+            raise ValueError(f"image {i}: {len(shp)} axes; 1 to 4 supported")
+        lv = levels[i]
+        lv = [int(lv)] * len(shp) if isinstance(lv, (int, np.integer)) else [int(v) for v in lv]
+        if len(lv) != len(shp) or min(lv) < 0:
+            raise ValueError(f"image {i}: levels {lv} for shape {shp}")
+        tab[i].wavelet = resolve_wavelet(wavelets[i])
+        tab[i].ndim = len(shp)
+        for d, v in enumerate(shp):
+            tab[i].shape[d] = v
+            tab[i].levels[d] = lv[d]
+        tab[i].in_offset = int(ino[i])
+        tab[i].out_offset = int(outo[i])
+    return tab, n
+
+
+def lwt_images(images, wavelets, levels=0, op=Transform.Forward, mode="Zero"):
+    """Transforms a list of CUDA tensors of differing shapes (each separable
+    over all of its axes, as ``pylifted`` would with ``axes=None``) in one C
+    ABI call on the current stream: the images are packed into one buffer,
+    identically shaped neighbours run as one launch per axis.  Returns the
+    list of results (views of one packed output)."""
+    torch = _torch()
+    if not images:
+        return []
+    dt = images[0].dtype
+    dev = images[0].device
+    for t in images:
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != dt or t.device != dev:
+            raise TypeError("images must be CUDA tensors of one dtype on one device")
+    shapes = [tuple(t.shape) for t in images]
+    flat = torch.cat([t.reshape(-1) for t in images])
+    out = torch.empty_like(flat)
+    tab, n = image_table(shapes, wavelets, levels)
+    lib = _lib.load()
+    fn = lib.lifted_lwt_batch_nd_f32 if _dtype_bytes(dt) == 4 else lib.lifted_lwt_batch_nd_f64
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(fn(int(op), resolve_mode(mode), n, ctypes.byref(tab), flat.data_ptr(),
+                      out.data_ptr(), stream))
+    res, off = [], 0
+    for shp in shapes:
+        sz = int(np.prod(shp))
+        res.append(out[off:off + sz].view(shp))
+        off += sz
+    return res
+
+
 def autotune(wavelets, length: int, op=Transform.Forward, mode="Zero",
              dtype="float32", total: int = 1 << 24):
     """Runs the native autotuner for each wavelet at this signal length."""
