@@ -329,6 +329,76 @@ def batched_section(dev, plain_sample: int = 300, steps: int = 5):
             "cpu_reference": cpu}
 
 
+def batched_nd_section(dev, steps: int = 10):
+    """Batched nD images of differing shapes: 48 float32 images (16 of
+    512^2, 16 of 256 x 1024, 8 of 1024^2, 8 of 384 x 640; N(0,1), seed
+    1006), CDF 9/7, 4 levels on both axes, Forward + ForwardAdjoint, each
+    transform one lifted_lwt_batch_nd_f32 call (graph replay), against one
+    separable call per image (the reference's loop of lifted::lwt calls)."""
+    import ctypes
+
+    import torch
+    from lifted_b200 import _lib
+    from lifted_b200 import pylifted as pl
+    from lifted_b200.batch import image_table
+
+    shapes = [(512, 512)] * 16 + [(256, 1024)] * 16 + [(1024, 1024)] * 8 + [(384, 640)] * 8
+    sizes = [a * b for a, b in shapes]
+    total = sum(sizes)
+    g = torch.Generator(device=dev).manual_seed(1006)
+    x = torch.randn(total, device=dev, generator=g)
+    w = torch.empty_like(x)
+    y = torch.empty_like(x)
+    tab, n = image_table(shapes, "cdf9.7", 4)
+    lib = _lib.load()
+
+    def step():
+        s = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(lib.lifted_lwt_batch_nd_f32(0, 0, n, ctypes.byref(tab), x.data_ptr(),
+                                               w.data_ptr(), s))
+        _lib.check(lib.lifted_lwt_batch_nd_f32(2, 0, n, ctypes.byref(tab), w.data_ptr(),
+                                               y.data_ptr(), s))
+
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    views = [(x[o:o + sz].view(shp), w[o:o + sz].view(shp), y[o:o + sz].view(shp))
+             for o, sz, shp in zip(offs, sizes, shapes)]
+
+    def plain():
+        for xi, wi, yi in views:
+            pl._lwt(xi, 100907, 0, 0, (0, 1), (4, 4), 1, out=wi)
+            pl._lwt(wi, 100907, 0, 2, (0, 1), (4, 4), 1, out=yi)
+
+    for _ in range(3):
+        step()
+        plain()
+    torch.cuda.synchronize(dev)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+        step()
+    graph.replay()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        plain()
+    torch.cuda.synchronize(dev)
+    ms_plain = (time.perf_counter() - t0) * 1e3 / steps
+    B = 2 * 2 * total * 4
+    return {"workload": "48 float32 images (16 x 512^2, 16 x 256x1024, 8 x 1024^2, 8 x "
+                        "384x640), CDF 9/7 4 levels on both axes, Forward + ForwardAdjoint",
+            "value": round(B / ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(ms, 4),
+            "cuda_graph": True,
+            "plain_per_image": {"value": round(B / ms_plain / 1e6, 3), "unit": "GB/s",
+                                "ms_per_step": round(ms_plain, 4),
+                                "sample": "one separable call per image and transform, wall clock"}}
+
+
 def inverse_section(dev, x, steps: int = 10):
     """Inverse + InverseAdjoint of the headline workload (the same kernels
     with the step order and signs of those transforms), timed as a CUDA
@@ -554,7 +624,8 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched, autograd and least-squares sections")
-    ap.add_argument("--section", choices=["inverse", "cfg1", "batched", "autograd", "lsq"],
+    ap.add_argument("--section", choices=["inverse", "cfg1", "batched", "batched_nd", "autograd",
+                                          "lsq"],
                     help="run only this section (one GPU) and print its JSON; for profiling "
                          "its kernels, not a driver line")
     args = ap.parse_args()
@@ -579,6 +650,7 @@ def main() -> int:
             res = inverse_section(dev, xi)
         else:
             fn = {"cfg1": cfg1_section, "batched": batched_section,
+                  "batched_nd": batched_nd_section,
                   "autograd": autograd_section, "lsq": lsq_section}[args.section]
             res = fn(dev)
         print(json.dumps({"section": args.section, **res}))
@@ -740,12 +812,13 @@ def main() -> int:
                              f"(reference sources + Highway stand-in, {variant}, "
                              f"{cores} threads)"}
 
-    extras = {"inverse": None, "cfg1_1d_f64": None, "batched": None, "autograd": None,
-              "lsq": None}
+    extras = {"inverse": None, "cfg1_1d_f64": None, "batched": None, "batched_nd": None,
+              "autograd": None, "lsq": None}
     if world == 1 and not args.no_extras:
         extras["inverse"] = inverse_section(dev, x)
         extras["cfg1_1d_f64"] = cfg1_section(dev)
         extras["batched"] = batched_section(dev)
+        extras["batched_nd"] = batched_nd_section(dev)
         extras["autograd"] = autograd_section(dev)
         extras["lsq"] = lsq_section(dev)
 
@@ -779,6 +852,7 @@ def main() -> int:
             "inverse": extras["inverse"],
             "cfg1_1d_f64": extras["cfg1_1d_f64"],
             "batched": extras["batched"],
+            "batched_nd": extras["batched_nd"],
             "autograd": extras["autograd"],
             "lsq": extras["lsq"],
         }
