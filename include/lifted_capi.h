@@ -319,6 +319,10 @@ LIFTED_CAPI uint64_t lifted_launch_count(void);
  *                               on the batch engine (many CTAs per line)
  *   "wrow_split"           0/1  float32 rows of 2048/4096 split over two
  *                               warps (else one warp per row)
+ *   "generic_kernels"      0/1  catalogue wavelets without compiled kernels
+ *                               run on the generic register kernels (each
+ *                               step dispatched on its shape) where they
+ *                               apply (else the general line kernel)
  *   "row_windows"          0/1  contiguous rows longer than one warp holds
  *                               run every level on windows with halos,
  *                               one warp each (else the batch engine)

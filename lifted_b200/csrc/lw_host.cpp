@@ -78,6 +78,7 @@ std::atomic<int64_t> g_opt_long_batched{1};
 std::atomic<int64_t> g_opt_wrow_split{1};
 std::atomic<int64_t> g_opt_overlap{1};
 std::atomic<int64_t> g_opt_row_windows{1};
+std::atomic<int64_t> g_opt_generic{1};
 
 }  // namespace
 
@@ -836,6 +837,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_overlap = value ? 1 : 0;
   } else if (!std::strcmp(name, "row_windows")) {
     g_opt_row_windows = value ? 1 : 0;
+  } else if (!std::strcmp(name, "generic_kernels")) {
+    g_opt_generic = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");
@@ -852,6 +855,7 @@ bool col_stacked() { return g_opt_tma_stacked.load() != 0; }
 bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
 bool pdl_enabled() { return g_opt_overlap.load() != 0; }
 bool wtile_enabled() { return g_opt_row_windows.load() != 0; }
+bool generic_enabled() { return g_opt_generic.load() != 0; }
 
 }  // namespace lw
 

@@ -104,6 +104,48 @@ constexpr int cat_reach(int wi, int op) {
   return r;
 }
 
+// The generic instantiation of the register kernels: one kernel for every
+// catalogue wavelet, each step dispatched at run time (DevStep::shape) to
+// the compiled code of its shape, out of the distinct (kind, target, offset,
+// taps, sign) shapes of all catalogue steps for that transform.
+constexpr int WI_GEN = 4096;
+constexpr int kNumCatalogue = (int)(sizeof(kRanges) / sizeof(kRanges[0]));
+constexpr int kMaxGenShapes = 96;
+
+struct GenShapes {
+  CStep s[kMaxGenShapes];
+  int n;
+};
+
+constexpr bool same_shape(const CStep& a, const CStep& b) {
+  return a.kind == b.kind && a.y_is_d == b.y_is_d && a.off == b.off && a.ntaps == b.ntaps &&
+         a.sub == b.sub;
+}
+
+constexpr GenShapes gen_shapes(int op) {
+  GenShapes g{};
+  g.n = 0;
+  for (int wi = 0; wi < kNumCatalogue; ++wi)
+    for (int k = 0; k < kRanges[wi].count; ++k) {
+      const CStep c = cstep(wi, op, k);
+      if (c.kind == K_SCALE) continue;
+      bool found = false;
+      for (int i = 0; i < g.n && !found; ++i) found = same_shape(g.s[i], c);
+      if (!found && g.n < kMaxGenShapes) g.s[g.n++] = c;
+    }
+  return g;
+}
+
+template <int OP>
+struct GenTable {
+  static constexpr GenShapes v = gen_shapes(OP);
+};
+
+// Reach of the level recursion (the generic kernels compile every level
+// down to one pair per chunk; the host bounds the levels by the actual
+// wavelet's reach) and register levels of an instantiation.
+constexpr int kreach(int wi, int op) { return wi == WI_GEN ? 1 : cat_reach(wi, op); }
+
 // Halo (pairs, per side) that one level of (wi, op) consumes.
 constexpr int cat_level_halo(int wi, int op) {
   int l = 0, r = 0;
@@ -494,7 +536,7 @@ __device__ __forceinline__ void rev_levels(VT (&s)[P0], VT (&d)[P0],
 // Number of levels the register path can run with P0 pairs per chunk.
 constexpr int reg_max_levels(int wi, int op, int p0) {
   int lv = 0;
-  const int reach = cat_reach(wi, op);
+  const int reach = kreach(wi, op);
   for (int p = p0; p >= 1 && p >= reach && lv < MAX_LEVELS; p >>= 1) ++lv;
   return lv;
 }

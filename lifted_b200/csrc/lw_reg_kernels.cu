@@ -46,6 +46,29 @@ bool compiled_wavelet(int wi) {
   return wi == WI_DB2 || wi == WI_DB4 || wi == WI_CDF97;
 }
 
+// Shape indices of a catalogue program's steps in the generic kernels'
+// table for transform `op`; false if a step has no compiled shape.
+template <typename T>
+bool set_gen_shapes(DevProgram<T>* p, int op) {
+  const GenShapes* g = op == 0 ? &GenTable<0>::v
+                     : op == 1 ? &GenTable<1>::v
+                     : op == 2 ? &GenTable<2>::v
+                               : &GenTable<3>::v;
+  for (int k = 0; k < p->nsteps; ++k) {
+    DevStep<T>& st = p->st[k];
+    st.shape = -1;
+    if (st.kind == K_SCALE) continue;
+    const CStep c{st.kind, st.y_is_d, st.off, st.ntaps, st.sub, 0, 0};
+    for (int i = 0; i < g->n; ++i)
+      if (same_shape(g->s[i], c)) {
+        st.shape = i;
+        break;
+      }
+    if (st.shape < 0) return false;
+  }
+  return true;
+}
+
 // The host-resolved program must have exactly the compile-time structure.
 template <typename T>
 bool structure_matches(const DevProgram<T>& prog, int wi, int op) {
@@ -184,9 +207,12 @@ template <typename T>
 int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   const LineGeom& g = a.g;
   if (!rows_vectorisable(g, a.in, a.out)) return 0;
+  // catalogue wavelets without a compiled kernel: the generic instantiation,
+  // every register level the wavelet's reach allows (no compacted levels)
+  const bool gen = !compiled_wavelet(a.wi);
   if constexpr (sizeof(T) == 4) {
     const int64_t q0 = g.n / 128;
-    if (wrow2_enabled() && g.n % 128 == 0 && (q0 == 16 || q0 == 32) &&
+    if (!gen && wrow2_enabled() && g.n % 128 == 0 && (q0 == 16 || q0 == 32) &&
         wrow2_levels_f32(a.wi, a.op, (int)q0) >= a.levels) {
       WRowParams<T> p;
       std::memset(&p, 0, sizeof(p));
@@ -210,8 +236,9 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   const int64_t p0 = g.n / 64;
   const int maxp0 = sizeof(T) == 4 ? 64 : 32;
   if (p0 < 8 || p0 > maxp0 || (p0 & (p0 - 1))) return 0;
-  const int lv = sizeof(T) == 4 ? wrow_levels_f32(a.wi, a.op, (int)p0)
-                                : wrow_levels_f64(a.wi, a.op, (int)p0);
+  const int lv = gen ? reg_max_levels(a.wi, a.op, (int)p0)
+                 : (sizeof(T) == 4 ? wrow_levels_f32(a.wi, a.op, (int)p0)
+                                   : wrow_levels_f64(a.wi, a.op, (int)p0));
   if (lv < a.levels) return 0;
   WRowParams<T> p;
   std::memset(&p, 0, sizeof(p));
@@ -220,6 +247,8 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   p.g = g;
   p.levels = a.levels;
   p.prog = *a.prog;
+  if (gen && !set_gen_shapes(&p.prog, a.op)) return 0;
+  const int wk = gen ? WI_GEN : a.wi;
   const int warps = 4;
   const size_t smem = (size_t)warps * (size_t)g.n * sizeof(T);
   if (smem > kMaxDynSmem) return 0;
@@ -227,9 +256,9 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   if (grid > 0x7fffffffLL) return 0;
   cudaError_t e;
   if constexpr (sizeof(T) == 4)
-    e = launch_wrow_f32(a.wi, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
+    e = launch_wrow_f32(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
   else
-    e = launch_wrow_f64(a.wi, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
+    e = launch_wrow_f64(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
   if (stats) stats->launches += 1;
   return 1;
@@ -697,11 +726,17 @@ template <typename T>
 int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
                   RegStats* stats) {
   if (a.bc != BC_ZERO) return 0;
-  if (a.wi < 0 || !compiled_wavelet(a.wi)) return 0;
+  if (a.wi < 0 || a.wi >= kNumCatalogue) return 0;
   if (a.levels < 1 || a.levels > MAX_LEVELS) return 0;
   if (!structure_matches(*a.prog, a.wi, a.op)) return 0;
   const LineGeom& g = a.g;
   const bool contiguous = (g.sin == 1 && g.sout == 1);
+  if (!compiled_wavelet(a.wi)) {
+    // the generic instantiation serves rows of 512-4096 (float32) or
+    // 512-2048 (float64) samples
+    if (!generic_enabled() || !contiguous) return 0;
+    return launch_wrow<T>(a, stream, stats);
+  }
   // whole lines: contiguous rows, or strided lines adjacent in memory
   if (contiguous) {
     int rc = launch_wrow<T>(a, stream, stats);

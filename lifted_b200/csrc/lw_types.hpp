@@ -46,6 +46,8 @@ struct DevStep {
   int32_t fold_off;
   int32_t nf;
   int32_t nb;
+  int32_t shape;   // index in the generic kernels' step-shape table (-1: none)
+  int32_t pad_;
   T c[MAX_TAPS];
   T sm;
   T dm;

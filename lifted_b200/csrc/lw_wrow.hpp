@@ -44,5 +44,8 @@ cudaError_t launch_wtile_f64(int wi, int op, const WTileParams<double>& p, int g
                              cudaStream_t stream);
 // Whether long contiguous rows may use it (the "row_windows" option).
 bool wtile_enabled();
+// Whether catalogue wavelets without compiled kernels may use the generic
+// instantiations (the "generic_kernels" option).
+bool generic_enabled();
 
 }  // namespace lw

@@ -46,6 +46,7 @@ Fn by_wavelet(int wi, int op) {
     case 2: return by_op<2, P0>(op);
     case 4: return by_op<4, P0>(op);
     case 33: return by_op<33, P0>(op);
+    case WI_GEN: return by_op<WI_GEN, P0>(op);
     default: return nullptr;
   }
 }

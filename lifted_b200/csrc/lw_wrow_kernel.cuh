@@ -171,10 +171,49 @@ __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
   }
 }
 
+// Generic kernels: the update of one step, dispatched on its shape index
+// (shapes reaching past P pairs are not compiled at this level; the host
+// never runs those levels).
+template <typename T, int OP, int P, int PA, int I>
+__device__ __forceinline__ void wgen_update(int shape, T (&s)[PA], T (&d)[PA],
+                                            const DevStep<T>& st, bool okl, bool okr) {
+  if constexpr (I < GenTable<OP>::v.n) {
+    if (shape == I) {
+      constexpr CStep cs = GenTable<OP>::v.s[I];
+      if constexpr (cs.left <= P && cs.right <= P) {
+        if constexpr (cs.y_is_d)
+          wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, okl,
+                                                                                  okr);
+        else
+          wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, okl,
+                                                                                  okr);
+      }
+      return;
+    }
+    wgen_update<T, OP, P, PA, I + 1>(shape, s, d, st, okl, okr);
+  }
+}
+
 template <typename T, int WI, int OP, int K, int P, int PA>
 __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
                                        const DevProgram<T>& prog, bool okl, bool okr) {
-  if constexpr (K < cat_nsteps(WI)) {
+  if constexpr (WI == WI_GEN) {
+    if constexpr (K == 0) {
+      for (int k = 0; k < prog.nsteps; ++k) {
+        const DevStep<T>& st = prog.st[k];
+        if (st.kind == K_SCALE) {
+          const T sm = st.sm, dm = st.dm;
+#pragma unroll
+          for (int i = 0; i < P; ++i) {
+            s[i] = s[i] * sm;
+            d[i] = d[i] * dm;
+          }
+        } else {
+          wgen_update<T, OP, P, PA, 0>(st.shape, s, d, st, okl, okr);
+        }
+      }
+    }
+  } else if constexpr (K < cat_nsteps(WI)) {
     constexpr CStep cs = cstep(WI, OP, K);
     const DevStep<T>& st = prog.st[K];
     if constexpr (cs.kind == K_SCALE) {
@@ -309,7 +348,7 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
                                      const DevProgram<T>& prog, int levels,
                                      int lane) {
   constexpr int P = P0 >> LV;
-  if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+  if constexpr (P >= 1 && P >= kreach(WI, OP)) {
     if (LV < levels) {
       constexpr int NB = 32 * P;  // band length at this level
       wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane > 0, lane < 31);
@@ -318,7 +357,7 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
         write_run<T, P, P>(buf, P * lane, s);
         return;
       }
-      if constexpr (LV + 1 >= reg_max_levels(WI, OP, P0)) {
+      if constexpr (WI != WI_GEN && LV + 1 >= reg_max_levels(WI, OP, P0)) {
         wcompact_fwd<T, WI, OP, P, P0>(s, buf, prog, levels, LV + 1, lane);
       } else {
 #pragma unroll
@@ -339,7 +378,7 @@ __device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
                                      int lane) {
   constexpr int P = P0 >> LV;
   if constexpr (LV >= 0) {
-    if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+    if constexpr (P >= 1 && P >= kreach(WI, OP)) {
       if (LV < levels) {
         constexpr int NB = 32 * P;
         if (LV + 1 == levels) read_run<T, P, P>(buf, P * lane, s);
@@ -427,8 +466,10 @@ __global__ void __launch_bounds__(128)
     wrow::wfwd<T, WI, OP, P0, 0>(s, d, buf, p.prog, p.levels, lane);
   } else {
     constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
-    if (p.levels > TOP + 1)
-      wrow::wcompact_rev<T, WI, OP, (P0 >> TOP), P0>(s, buf, p.prog, p.levels, TOP + 1, lane);
+    if constexpr (WI != WI_GEN) {
+      if (p.levels > TOP + 1)
+        wrow::wcompact_rev<T, WI, OP, (P0 >> TOP), P0>(s, buf, p.prog, p.levels, TOP + 1, lane);
+    }
     wrow::wrev<T, WI, OP, P0, TOP>(s, d, buf, p.prog, p.levels, lane);
     __syncwarp();
     T x[2 * P0];

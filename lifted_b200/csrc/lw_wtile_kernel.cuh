@@ -99,7 +99,7 @@ template <typename T, int WI, int OP, int P0, int LV>
 __device__ __forceinline__ void fwd(T (&s)[P0], T (&d)[P0], T* buf, const DevProgram<T>& prog,
                                     int levels, int lane, int64_t wstart, int64_t n) {
   constexpr int P = P0 >> LV;
-  if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+  if constexpr (P >= 1 && P >= kreach(WI, OP)) {
     if (LV < levels) {
       constexpr int NB = 32 * P;
       const int64_t nbp = n >> (LV + 1);                 // pairs of the row's band
@@ -126,7 +126,7 @@ __device__ __forceinline__ void rev(T (&s)[P0], T (&d)[P0], T* buf, const DevPro
                                     int levels, int lane, int64_t wstart, int64_t n) {
   constexpr int P = P0 >> LV;
   if constexpr (LV >= 0) {
-    if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+    if constexpr (P >= 1 && P >= kreach(WI, OP)) {
       if (LV < levels) {
         constexpr int NB = 32 * P;
         const int64_t nbp = n >> (LV + 1);
