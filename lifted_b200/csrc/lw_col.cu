@@ -43,6 +43,7 @@ ColFn<T> by_wavelet(int wi, int op) {
     case 2: return by_op<T, 2, V>(op);
     case 4: return by_op<T, 4, V>(op);
     case 33: return by_op<T, 33, V>(op);
+    case WI_GEN: return by_op<T, WI_GEN, V>(op);
     default: return nullptr;
   }
 }

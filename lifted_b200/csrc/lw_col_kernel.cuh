@@ -215,7 +215,7 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
   // the level after whose reads the staging buffer is free
   constexpr int LAST_READ = preload_d1<T>() ? 1 : 0;
   if constexpr (LV >= 0) {
-    if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+    if constexpr (P >= 1 && P >= kreach(WI, OP)) {
       const int k = c.p->nreg;
       if (LV < k) {
         const RegParams<T>& p = *c.p;
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   static_assert(V == 1 || sizeof(T) == 4, "packed lanes are float32 only");
   constexpr int P0 = COL_P0;
   constexpr int W = COL_LANES * V;
-  constexpr int HMAX = cat_reach(WI, OP) > 0 ? cat_reach(WI, OP) : 1;
+  constexpr int HMAX = khmax(WI, OP);
   constexpr bool FWD = (OP == TF_F || OP == TF_IA);
   extern __shared__ __align__(128) unsigned char col_smem[];
   T* stage = reinterpret_cast<T*>(col_smem);

@@ -145,6 +145,13 @@ struct GenTable {
 // down to one pair per chunk; the host bounds the levels by the actual
 // wavelet's reach) and register levels of an instantiation.
 constexpr int kreach(int wi, int op) { return wi == WI_GEN ? 1 : cat_reach(wi, op); }
+// Neighbour-exchange width of the block-level register kernels: the
+// wavelet's reach, or for the generic instantiation a fixed width (wavelets
+// of larger reach stay on the general kernel there).
+constexpr int kGenHmax = 5;
+constexpr int khmax(int wi, int op) {
+  return wi == WI_GEN ? kGenHmax : (cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1);
+}
 
 // Halo (pairs, per side) that one level of (wi, op) consumes.
 constexpr int cat_level_halo(int wi, int op) {
@@ -336,11 +343,52 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
   }
 }
 
+// Generic instantiation: one step's update dispatched on its shape index
+// (shapes wider than P pairs or than the exchange width are not compiled;
+// the host never runs them).  Every thread takes the same branch.
+template <typename T, typename VT, int OP, int P, int PA, int HMAX, int I>
+__device__ __forceinline__ void gen_update(int shape, VT (&s)[PA], VT (&d)[PA],
+                                           const DevStep<T>& st, Ctx<T>& c, int64_t gp0,
+                                           int64_t nb) {
+  if constexpr (I < GenTable<OP>::v.n) {
+    if (shape == I) {
+      constexpr CStep cs = GenTable<OP>::v.s[I];
+      if constexpr (cs.left <= P && cs.right <= P && cs.left <= HMAX && cs.right <= HMAX) {
+        if constexpr (cs.y_is_d)
+          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(
+              d, s, st, c, gp0, nb);
+        else
+          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(
+              s, d, st, c, gp0, nb);
+      }
+      return;
+    }
+    gen_update<T, VT, OP, P, PA, HMAX, I + 1>(shape, s, d, st, c, gp0, nb);
+  }
+}
+
 template <typename T, typename VT, int WI, int OP, int K, int P, int PA,
           int HMAX>
 __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
                                       int64_t gp0, int64_t nb) {
-  if constexpr (K < cat_nsteps(WI)) {
+  if constexpr (WI == WI_GEN) {
+    if constexpr (K == 0) {
+      const DevProgram<T>& prog = c.p->prog;
+      for (int k = 0; k < prog.nsteps; ++k) {
+        const DevStep<T>& st = prog.st[k];
+        if (st.kind == K_SCALE) {
+          const T sm = st.sm, dm = st.dm;
+#pragma unroll
+          for (int i = 0; i < P; ++i) {
+            s[i] = vmul(s[i], sm);
+            d[i] = vmul(d[i], dm);
+          }
+        } else {
+          gen_update<T, VT, OP, P, PA, HMAX, 0>(st.shape, s, d, st, c, gp0, nb);
+        }
+      }
+    }
+  } else if constexpr (K < cat_nsteps(WI)) {
     constexpr CStep cs = cstep(WI, OP, K);
     const DevStep<T>& st = c.p->prog.st[K];
     if constexpr (cs.kind == K_SCALE) {
@@ -401,7 +449,7 @@ template <typename T, typename VT, int V, int WI, int OP, int P0, int HMAX,
 __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
                                            Ctx<T>& c) {
   constexpr int P = P0 >> LV;
-  if constexpr (P >= 1 && P >= cat_reach(WI, OP) && LV < MAX_LEVELS) {
+  if constexpr (P >= 1 && P >= kreach(WI, OP) && LV < MAX_LEVELS) {
     if (LV < c.p->nreg) {
       const int64_t nb = c.n >> (LV + 1);
       const int64_t gp0 = c.e0 >> (LV + 1);
@@ -448,7 +496,7 @@ __device__ __forceinline__ void rev_levels(VT (&s)[P0], VT (&d)[P0],
                                            Ctx<T>& c) {
   constexpr int P = P0 >> LV;
   if constexpr (LV >= 0) {
-    if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
+    if constexpr (P >= 1 && P >= kreach(WI, OP)) {
       if (LV < c.p->nreg) {
         const RegParams<T>& p = *c.p;
         const int64_t nb = c.n >> (LV + 1);
@@ -548,7 +596,7 @@ __global__ void __launch_bounds__(512)
     reg_kernel(const __grid_constant__ RegParams<T> p) {
   using VT = typename LaneVec<T, V>::type;
   static_assert(V == 1 || STRIDED, "vector lanes need the strided mapping");
-  constexpr int HMAX = cat_reach(WI, OP) > 0 ? cat_reach(WI, OP) : 1;
+  constexpr int HMAX = khmax(WI, OP);
   constexpr bool FWD = (OP == TF_F || OP == TF_IA);
   extern __shared__ __align__(16) unsigned char lw_reg_smem[];
   pdl_wait();  // the previous kernel's results (no global access before)

@@ -551,9 +551,15 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // packed lanes only while they still give every SM a tile
     if (v == 2 && ncols / (2 * COL_LANES) * ntr * ngroups < sm_count())
       v = 1;
+    // catalogue wavelets without compiled kernels: the generic instantiation
+    // (reach up to its exchange width), and the band levels must fit one
+    // more launch of it
+    const bool gen = !compiled_wavelet(wi);
+    if (gen && (cat_reach(wi, op) > kGenHmax || a.levels - k > maxreg)) return 0;
+    const int wk = gen ? WI_GEN : wi;
     ColFn<T> fn;
-    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wi, op, v);
-    else fn = pick_col_f64(wi, op);
+    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v);
+    else fn = pick_col_f64(wk, op);
     if (!fn) return 0;
     const int64_t m = n >> k;
     const bool more = a.levels > k;
@@ -624,6 +630,10 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     r.halo = halo;
     r.ntiles = ntr;
     r.prog = *a.prog;
+    if (gen && !set_gen_shapes(&r.prog, op)) {
+      if (tmp) scratch_free(tmp, stream);
+      return 0;
+    }
     cp.ncols = ncols;
     cp.nouter = nouter;
     cp.ntr = ntr;
@@ -633,7 +643,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     cp.a_from_tmp = more ? 1 : 0;
     cp.spin_limit = 1 << 22;
     cp.err = err;
-    const int hmax = cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1;
+    const int hmax = gen ? kGenHmax : (cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1);
     const size_t smem = col_smem_bytes(hmax, v, EB);
     if (smem > kMaxDynSmem) {
       if (tmp) scratch_free(tmp, stream);
@@ -732,10 +742,12 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
   const LineGeom& g = a.g;
   const bool contiguous = (g.sin == 1 && g.sout == 1);
   if (!compiled_wavelet(a.wi)) {
-    // the generic instantiation serves rows of 512-4096 (float32) or
-    // 512-2048 (float64) samples
-    if (!generic_enabled() || !contiguous) return 0;
-    return launch_wrow<T>(a, stream, stats);
+    // the generic instantiations: rows of 512-4096 (float32) or 512-2048
+    // (float64) samples, strided lines adjacent in memory
+    if (!generic_enabled()) return 0;
+    if (contiguous) return launch_wrow<T>(a, stream, stats);
+    if (lines_adjacent(g)) return launch_col<T>(a, stream, stats);
+    return 0;
   }
   // whole lines: contiguous rows, or strided lines adjacent in memory
   if (contiguous) {
