@@ -293,13 +293,16 @@ int launch_wtile(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) 
   p.ntiles = (n + tile - 1) / tile;
   p.levels = a.levels;
   p.prog = *a.prog;
+  const bool gen = !compiled_wavelet(a.wi);
+  if (gen && !set_gen_shapes(&p.prog, a.op)) return 0;
+  const int wk = gen ? WI_GEN : a.wi;
   const int warps = 4;
   const int64_t grid = (g.nlines * p.ntiles + warps - 1) / warps;
   if (grid > 0x7fffffffLL) return 0;
   const size_t smem = (size_t)warps * (size_t)W * sizeof(T);
   cudaError_t e;
-  if constexpr (sizeof(T) == 4) e = launch_wtile_f32(a.wi, a.op, p, (int)grid, smem, stream);
-  else e = launch_wtile_f64(a.wi, a.op, p, (int)grid, smem, stream);
+  if constexpr (sizeof(T) == 4) e = launch_wtile_f32(wk, a.op, p, (int)grid, smem, stream);
+  else e = launch_wtile_f64(wk, a.op, p, (int)grid, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
   if (stats) stats->launches += 1;
   return 1;
@@ -745,7 +748,11 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
     // the generic instantiations: rows of 512-4096 (float32) or 512-2048
     // (float64) samples, strided lines adjacent in memory
     if (!generic_enabled()) return 0;
-    if (contiguous) return launch_wrow<T>(a, stream, stats);
+    if (contiguous) {
+      const int rc = launch_wrow<T>(a, stream, stats);
+      if (rc != 0) return rc;
+      return launch_wtile<T>(a, stream, stats);
+    }
     if (lines_adjacent(g)) return launch_col<T>(a, stream, stats);
     return 0;
   }

@@ -48,6 +48,7 @@ Fn<T> by_wavelet(int wi, int op) {
     case 2: return by_op<T, 2, P0>(op);
     case 4: return by_op<T, 4, P0>(op);
     case 33: return by_op<T, 33, P0>(op);
+    case WI_GEN: return by_op<T, WI_GEN, P0>(op);
     default: return nullptr;
   }
 }
@@ -57,7 +58,9 @@ Fn<T> by_wavelet(int wi, int op) {
 int wtile_pairs(int elem_bytes) { return elem_bytes == 4 ? 32 : 16; }
 
 int wtile_levels(int wi, int op, int elem_bytes) {
-  if (wi != 2 && wi != 4 && wi != 33) return 0;
+  // every catalogue wavelet: compiled ones directly, the others through the
+  // generic instantiation
+  if (wi < 0 || wi >= kNumCatalogue) return 0;
   return reg_max_levels(wi, op, wtile_pairs(elem_bytes));
 }
 

@@ -72,3 +72,22 @@ def test_all_catalogue_wavelets_strided(op, dtype):
             g, _ = run(x, w, op, axes, lv)
             assert np.array_equal(g, o), (w, shape, axes, lv)
     assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_all_catalogue_wavelets_long_rows(op, dtype):
+    """Rows longer than one warp holds on the generic windowed kernel (first,
+    last and shorter windows clipped by the row): every catalogue wavelet."""
+    rng = np.random.default_rng(99 + op)
+    for w in po.wavelet_values():
+        width = po.wavelet_width(w)
+        n = 12288
+        mx = po.max_level(width, n) if width > 1 else int(np.log2(n))
+        for lv in sorted({1, max(1, min(3, mx))}):
+            x = rng.standard_normal((2, n)).astype(dtype)
+            rc, o = po.oracle_sep(x, w, op, 0, [1], [lv])
+            if rc:
+                continue
+            g, _ = run(x, w, op, [1], [lv])
+            assert np.array_equal(g, o), (w, n, lv)
