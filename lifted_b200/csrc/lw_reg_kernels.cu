@@ -236,10 +236,18 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   const int64_t p0 = g.n / 64;
   const int maxp0 = sizeof(T) == 4 ? 64 : 32;
   if (p0 < 8 || p0 > maxp0 || (p0 & (p0 - 1))) return 0;
-  const int lv = gen ? reg_max_levels(a.wi, a.op, (int)p0)
-                 : (sizeof(T) == 4 ? wrow_levels_f32(a.wi, a.op, (int)p0)
-                                   : wrow_levels_f64(a.wi, a.op, (int)p0));
-  if (lv < a.levels) return 0;
+  // generic: the wavelet's register levels, then compacted lanes of 16
+  // pairs each, halving per level down to one lane
+  const int lc = gen ? reg_max_levels(a.wi, a.op, (int)p0) : 0;
+  int lv;
+  if (gen) {
+    lv = lc;
+    if (lc >= 1)
+      for (int64_t act = (int64_t)p0 >> (lc - 1); act >= 1; act >>= 1) ++lv;
+  } else {
+    lv = sizeof(T) == 4 ? wrow_levels_f32(a.wi, a.op, (int)p0) : wrow_levels_f64(a.wi, a.op, (int)p0);
+  }
+  if (lc < 0 || lv < a.levels || (gen && lc < 1)) return 0;
   WRowParams<T> p;
   std::memset(&p, 0, sizeof(p));
   p.in = a.in;
@@ -248,6 +256,7 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   p.levels = a.levels;
   p.prog = *a.prog;
   if (gen && !set_gen_shapes(&p.prog, a.op)) return 0;
+  p.reg_levels = lc;
   const int wk = gen ? WI_GEN : a.wi;
   const int warps = 4;
   const size_t smem = (size_t)warps * (size_t)g.n * sizeof(T);

@@ -33,8 +33,9 @@ struct WRowParams {
   const T* in;
   T* out;
   LineGeom g;        // contiguous rows (g.sin == g.sout == 1)
-  int32_t levels;    // all levels run in registers
-  int32_t pad_;
+  int32_t levels;      // levels of the pass
+  int32_t reg_levels;  // generic instantiation: levels in registers (the
+                       // rest on compacted lanes); unused otherwise
   DevProgram<T> prog;
 };
 
@@ -246,7 +247,11 @@ constexpr int pow2_at_least(int r) {
 }
 template <int WI, int OP>
 constexpr int compact_pairs() {
-  return pow2_at_least(cat_reach(WI, OP) > 1 ? cat_reach(WI, OP) : 1);
+  if constexpr (WI == WI_GEN) {
+    return 16;  // covers every catalogue reach
+  } else {
+    return pow2_at_least(cat_reach(WI, OP) > 1 ? cat_reach(WI, OP) : 1);
+  }
 }
 
 // Active lanes take 2*PC consecutive elements (written with run length
@@ -346,7 +351,7 @@ __device__ __forceinline__ void wcompact_rev(T (&s)[PA], T* buf, const DevProgra
 template <typename T, int WI, int OP, int P0, int LV>
 __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
                                      const DevProgram<T>& prog, int levels,
-                                     int lane) {
+                                     int lane, int lc) {
   constexpr int P = P0 >> LV;
   if constexpr (P >= 1 && P >= kreach(WI, OP)) {
     if (LV < levels) {
@@ -357,7 +362,19 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
         write_run<T, P, P>(buf, P * lane, s);
         return;
       }
-      if constexpr (WI != WI_GEN && LV + 1 >= reg_max_levels(WI, OP, P0)) {
+      if constexpr (WI == WI_GEN) {
+        // the wavelet's register levels end at lc (run time)
+        if (LV + 1 >= lc) {
+          wcompact_fwd<T, WI, OP, P, P0>(s, buf, prog, levels, LV + 1, lane);
+          return;
+        }
+#pragma unroll
+        for (int i = 0; i < P / 2; ++i) {
+          d[i] = s[2 * i + 1];
+          s[i] = s[2 * i];
+        }
+        wfwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane, lc);
+      } else if constexpr (LV + 1 >= reg_max_levels(WI, OP, P0)) {
         wcompact_fwd<T, WI, OP, P, P0>(s, buf, prog, levels, LV + 1, lane);
       } else {
 #pragma unroll
@@ -365,7 +382,7 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
           d[i] = s[2 * i + 1];
           s[i] = s[2 * i];
         }
-        wfwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane);
+        wfwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane, lc);
       }
     }
   }
@@ -375,11 +392,12 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
 template <typename T, int WI, int OP, int P0, int LV>
 __device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
                                      const DevProgram<T>& prog, int levels,
-                                     int lane) {
+                                     int lane, int lc) {
   constexpr int P = P0 >> LV;
   if constexpr (LV >= 0) {
     if constexpr (P >= 1 && P >= kreach(WI, OP)) {
-      if (LV < levels) {
+      // generic: levels at and past lc ran on compacted lanes
+      if (LV < levels && (WI != WI_GEN || LV < lc)) {
         constexpr int NB = 32 * P;
         if (LV + 1 == levels) read_run<T, P, P>(buf, P * lane, s);
         read_run<T, P, P>(buf, NB + P * lane, d);
@@ -393,7 +411,22 @@ __device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
         }
       }
     }
-    if constexpr (LV > 0) wrev<T, WI, OP, P0, LV - 1>(s, d, buf, prog, levels, lane);
+    if constexpr (LV > 0) wrev<T, WI, OP, P0, LV - 1>(s, d, buf, prog, levels, lane, lc);
+  }
+}
+
+// Generic instantiation: the compacted reverse levels above register
+// level lc (run time), dispatched to the instantiation for its pair count.
+template <typename T, int WI, int OP, int P0, int L>
+__device__ __forceinline__ void gen_compact_rev(int lc, T (&s)[P0], T* buf,
+                                                const DevProgram<T>& prog, int levels,
+                                                int lane) {
+  if constexpr ((P0 >> L) >= 1) {
+    if (lc - 1 == L) {
+      wcompact_rev<T, WI, OP, (P0 >> L), P0>(s, buf, prog, levels, lc, lane);
+      return;
+    }
+    gen_compact_rev<T, WI, OP, P0, L + 1>(lc, s, buf, prog, levels, lane);
   }
 }
 
@@ -463,14 +496,17 @@ __global__ void __launch_bounds__(128)
       d[i] = x[2 * i + 1];
     }
     __syncwarp();
-    wrow::wfwd<T, WI, OP, P0, 0>(s, d, buf, p.prog, p.levels, lane);
+    wrow::wfwd<T, WI, OP, P0, 0>(s, d, buf, p.prog, p.levels, lane, p.reg_levels);
   } else {
     constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
     if constexpr (WI != WI_GEN) {
       if (p.levels > TOP + 1)
         wrow::wcompact_rev<T, WI, OP, (P0 >> TOP), P0>(s, buf, p.prog, p.levels, TOP + 1, lane);
+    } else {
+      if (p.levels > p.reg_levels && p.reg_levels >= 1)
+        wrow::gen_compact_rev<T, WI, OP, P0, 0>(p.reg_levels, s, buf, p.prog, p.levels, lane);
     }
-    wrow::wrev<T, WI, OP, P0, TOP>(s, d, buf, p.prog, p.levels, lane);
+    wrow::wrev<T, WI, OP, P0, TOP>(s, d, buf, p.prog, p.levels, lane, p.reg_levels);
     __syncwarp();
     T x[2 * P0];
 #pragma unroll
