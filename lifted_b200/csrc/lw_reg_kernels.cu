@@ -498,6 +498,64 @@ template <typename T>
 int band_pass(const RegPassArgs<T>& a, const LineGeom& g2, const T* in, T* out, int levels,
               cudaStream_t stream, RegStats* stats);
 
+// Levels of one launch of the TMA-staged kernel on lines of n samples and
+// its window geometry: whole lines of up to 512 (k = the register levels,
+// fewer when the band must again be a multiple of 32 long), or 512-sample
+// windows with halos (the smallest k whose band fits whole lines, else the
+// register levels).
+template <typename T>
+bool col_levels_plan(int wi, int op, int64_t n, int levels, int* k_out, int64_t* tile,
+                     int64_t* halo, int64_t* ntr) {
+  const int maxreg = std::min(reg_max_levels(wi, op, COL_P0), COL_MAXK);
+  int k = 0;
+  if (n <= COL_ROWS) {
+    k = std::min(levels, maxreg);
+    // levels past k run on the approximation band: on the whole-line
+    // register kernel when its lines fit one (n <= 32 * p0), else here
+    // again, which needs band lines a multiple of 32 long (float64 lines
+    // of 512 with more levels than the registers hold)
+    if (levels > k && n / (2 * p0_of<T>()) > 16)
+      while (k > 0 && ((n >> k) % 32)) --k;
+    *tile = n;
+    *halo = 0;
+    *ntr = 1;
+  } else {
+    for (int kk = 1; kk <= maxreg && kk <= levels; ++kk) {
+      k = kk;
+      const int64_t m = n >> kk;
+      if (m % 32 == 0 && m / 32 <= 16) break;
+    }
+    int64_t need = 0;
+    const int lh = cat_level_halo(wi, op);
+    for (int l = 1; l <= k; ++l) need += (int64_t)lh << l;
+    *halo = (need + 31) / 32 * 32;
+    *tile = COL_ROWS - 2 * *halo;
+    if (*tile < 128) return false;
+    *ntr = (n + *tile - 1) / *tile;
+  }
+  *k_out = k;
+  return k >= 1;
+}
+
+// Whether a pass of `levels` levels on lines of n samples runs through to
+// the end as a chain of launches of the TMA-staged kernel (each later one on
+// the previous one's approximation band; windowed bands chain again), or,
+// for compiled wavelets, ends on the whole-line register kernel.  Checked
+// before the first launch, so no launch is left without its band pass.
+template <typename T>
+bool col_chain_ok(int wi, int op, int64_t n, int levels, int depth) {
+  if (depth > 8 || n % 32) return false;
+  int k;
+  int64_t tile, halo, ntr;
+  if (!col_levels_plan<T>(wi, op, n, levels, &k, &tile, &halo, &ntr)) return false;
+  if (levels == k) return true;
+  const int64_t m = n >> k;
+  if (m % 32) return false;
+  if (col_chain_ok<T>(wi, op, m, levels - k, depth + 1)) return true;
+  constexpr int P0 = p0_of<T>();
+  return compiled_wavelet(wi) && m % (2 * P0) == 0 && m / (2 * P0) <= 16;
+}
+
 // Strided float32 pass on the TMA-staged persistent kernel: whole lines of
 // up to 512 samples, or 512-sample windows with halos on longer lines; the
 // levels beyond the first k run as a strided whole-line launch on the
@@ -523,36 +581,10 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (EB == 4 && col_packed() && ncols % (2 * COL_LANES) == 0 && (g.sout % 2) == 0 &&
         (g.nother < 2 || (g.oout[1] % 2) == 0) && (reinterpret_cast<uintptr_t>(a.out) & 7) == 0)
       v = 2;
-    const int maxreg = std::min(reg_max_levels(wi, op, COL_P0), COL_MAXK);
+    if (n > COL_ROWS && a.in_place) return 0;  // windows would overwrite other windows' input
     int k = 0;
     int64_t tile, halo, ntr;
-    if (n <= COL_ROWS) {
-      k = std::min(a.levels, maxreg);
-      // levels past k run on the approximation band: on the whole-line
-      // register kernel when its lines fit one (n <= 32 * p0), else here
-      // again, which needs band lines a multiple of 32 long (float64 lines
-      // of 512 with more levels than the registers hold)
-      if (a.levels > k && n / (2 * p0_of<T>()) > 16)
-        while (k > 0 && ((n >> k) % 32)) --k;
-      tile = n;
-      halo = 0;
-      ntr = 1;
-    } else {
-      if (a.in_place) return 0;  // windows would overwrite other windows' input
-      for (int kk = 1; kk <= maxreg && kk <= a.levels; ++kk) {
-        k = kk;
-        const int64_t m = n >> kk;
-        if (m % 32 == 0 && m / 32 <= 16) break;
-      }
-      int64_t need = 0;
-      const int lh = cat_level_halo(wi, op);
-      for (int l = 1; l <= k; ++l) need += (int64_t)lh << l;
-      halo = (need + 31) / 32 * 32;
-      tile = COL_ROWS - 2 * halo;
-      if (tile < 128) return 0;
-      ntr = (n + tile - 1) / tile;
-    }
-    if (k < 1) return 0;
+    if (!col_levels_plan<T>(wi, op, n, a.levels, &k, &tile, &halo, &ntr)) return 0;
     const int64_t nouter = g.nother == 2 ? g.oshape[1] : 1;
     // short whole lines of a 3D view: a tile stacks 512/n consecutive outer
     // slices (the staging window stays full)
@@ -567,7 +599,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // (reach up to its exchange width), and the band levels must fit one
     // more launch of it
     const bool gen = !compiled_wavelet(wi);
-    if (gen && (cat_reach(wi, op) > kGenHmax || a.levels - k > maxreg)) return 0;
+    if (gen && cat_reach(wi, op) > kGenHmax) return 0;
     const int wk = gen ? WI_GEN : wi;
     ColFn<T> fn;
     if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v);
@@ -575,7 +607,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (!fn) return 0;
     const int64_t m = n >> k;
     const bool more = a.levels > k;
-    if (more && ((m % 32) || m / 32 > 16)) return 0;
+    if (more && !col_chain_ok<T>(wi, op, n, a.levels, 0)) return 0;
     if (!more && a.levels != k) return 0;
     int32_t* err = col_error_flag();
     if (!err) return 0;

@@ -134,7 +134,8 @@ def test_tma_long_strided_lines(op, dtype):
     lines per lane, a 3D view and more levels than the band launch holds in
     registers: bit for bit against the oracle."""
     rng = np.random.default_rng(40 + op)
-    cases = [((4096, 2048), [0], [6]), ((2048, 32, 64), [0], [5]), ((4096, 64), [0], [9])]
+    cases = [((4096, 2048), [0], [6]), ((2048, 32, 64), [0], [5]), ((4096, 64), [0], [9]),
+             ((16384, 64), [0], [7]), ((8192, 32, 32), [0], [6])]
     for w in WAVELETS:
         for shape, axes, lv in cases:
             x = rng.standard_normal(shape).astype(dtype)

@@ -56,7 +56,8 @@ def test_all_catalogue_wavelets_strided(op, dtype):
     columns on windows plus a band launch, short lines of a 3D view stacked
     per window, and a 2D separable transform; every catalogue wavelet."""
     rng = np.random.default_rng(95 + op)
-    cases = [((512, 64), [0]), ((2048, 64), [0]), ((64, 8, 64), [0]), ((256, 96), [0, 1])]
+    cases = [((512, 64), [0]), ((2048, 64), [0]), ((64, 8, 64), [0]), ((256, 96), [0, 1]),
+             ((8192, 32), [0])]
     for w in po.wavelet_values():
         width = po.wavelet_width(w)
         for shape, axes in cases:
@@ -64,7 +65,7 @@ def test_all_catalogue_wavelets_strided(op, dtype):
             for a in axes:
                 n = shape[a]
                 mx = po.max_level(width, n) if width > 1 else int(np.log2(n))
-                lv.append(max(1, min(4, mx)))
+                lv.append(max(1, min(6 if n > 4096 else 4, mx)))
             x = rng.standard_normal(shape).astype(dtype)
             rc, o = po.oracle_sep(x, w, op, 0, axes, lv)
             if rc:
