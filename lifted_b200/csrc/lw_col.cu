@@ -44,6 +44,9 @@ ColFn<T> by_wavelet(int wi, int op) {
     case 4: return by_op<T, 4, V>(op);
     case 33: return by_op<T, 33, V>(op);
     case WI_GEN: return by_op<T, WI_GEN, V>(op);
+    case WI_GENW:
+      if constexpr (sizeof(T) == 4 && V == 1) return by_op<T, WI_GENW, V>(op);
+      else return nullptr;
     default: return nullptr;
   }
 }

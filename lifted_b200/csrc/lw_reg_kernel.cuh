@@ -109,6 +109,10 @@ constexpr int cat_reach(int wi, int op) {
 // the compiled code of its shape, out of the distinct (kind, target, offset,
 // taps, sign) shapes of all catalogue steps for that transform.
 constexpr int WI_GEN = 4096;
+// A second generic instantiation of the block-level kernels with a wider
+// neighbour exchange (float32 strided passes of wavelets of reach 6-9).
+constexpr int WI_GENW = 4097;
+constexpr bool is_gen(int wi) { return wi == WI_GEN || wi == WI_GENW; }
 constexpr int kNumCatalogue = (int)(sizeof(kRanges) / sizeof(kRanges[0]));
 constexpr int kMaxGenShapes = 96;
 
@@ -144,13 +148,16 @@ struct GenTable {
 // Reach of the level recursion (the generic kernels compile every level
 // down to one pair per chunk; the host bounds the levels by the actual
 // wavelet's reach) and register levels of an instantiation.
-constexpr int kreach(int wi, int op) { return wi == WI_GEN ? 1 : cat_reach(wi, op); }
+constexpr int kreach(int wi, int op) { return is_gen(wi) ? 1 : cat_reach(wi, op); }
 // Neighbour-exchange width of the block-level register kernels: the
 // wavelet's reach, or for the generic instantiation a fixed width (wavelets
 // of larger reach stay on the general kernel there).
 constexpr int kGenHmax = 5;
+constexpr int kGenWideHmax = 9;
 constexpr int khmax(int wi, int op) {
-  return wi == WI_GEN ? kGenHmax : (cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1);
+  return wi == WI_GEN    ? kGenHmax
+         : wi == WI_GENW ? kGenWideHmax
+                         : (cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1);
 }
 
 // Halo (pairs, per side) that one level of (wi, op) consumes.
@@ -371,7 +378,7 @@ template <typename T, typename VT, int WI, int OP, int K, int P, int PA,
           int HMAX>
 __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
                                       int64_t gp0, int64_t nb) {
-  if constexpr (WI == WI_GEN) {
+  if constexpr (is_gen(WI)) {
     if constexpr (K == 0) {
       const DevProgram<T>& prog = c.p->prog;
       for (int k = 0; k < prog.nsteps; ++k) {

@@ -599,8 +599,12 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // (reach up to its exchange width), and the band levels must fit one
     // more launch of it
     const bool gen = !compiled_wavelet(wi);
-    if (gen && cat_reach(wi, op) > kGenHmax) return 0;
-    const int wk = gen ? WI_GEN : wi;
+    // reach above the generic exchange width: the wide instantiation
+    // (float32, one line per lane)
+    const bool wide = gen && cat_reach(wi, op) > kGenHmax;
+    if (wide && (EB != 4 || cat_reach(wi, op) > kGenWideHmax)) return 0;
+    if (wide) v = 1;
+    const int wk = wide ? WI_GENW : (gen ? WI_GEN : wi);
     ColFn<T> fn;
     if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v);
     else fn = pick_col_f64(wk, op);
@@ -687,7 +691,9 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     cp.a_from_tmp = more ? 1 : 0;
     cp.spin_limit = 1 << 22;
     cp.err = err;
-    const int hmax = gen ? kGenHmax : (cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1);
+    const int hmax = wide ? kGenWideHmax
+                     : gen ? kGenHmax
+                           : (cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1);
     const size_t smem = col_smem_bytes(hmax, v, EB);
     if (smem > kMaxDynSmem) {
       if (tmp) scratch_free(tmp, stream);
