@@ -399,6 +399,55 @@ def batched_nd_section(dev, steps: int = 10):
                                 "sample": "one separable call per image and transform, wall clock"}}
 
 
+def generic_section(dev, steps: int = 10):
+    """Catalogue wavelets without compiled kernels (the generic register
+    instantiations): 4096^2 float32 2D separable transforms, levels (4, 4),
+    Forward + ForwardAdjoint, graph-replayed, for three such wavelets, and
+    the same steps on the general line kernel (option off) beside them."""
+    import torch
+    from lifted_b200 import _lib
+    from lifted_b200 import pylifted as pl
+
+    g = torch.Generator(device=dev).manual_seed(1007)
+    x = torch.randn(4096, 4096, device=dev, generator=g)
+    w = torch.empty_like(x)
+    y = torch.empty_like(x)
+    B = 2 * 2 * x.numel() * 4
+    out = {"workload": "4096^2 float32 N(0,1) (seed 1007), levels (4, 4) on axes (0, 1), "
+                       "Zero boundary, Forward + ForwardAdjoint", "unit": "GB/s"}
+    for wv in (5, 104, 7):
+        res = {}
+        for on in (1, 0):
+            _lib.set_option("generic_kernels", on)
+            try:
+                def step():
+                    pl._lwt(x, wv, 0, 0, (0, 1), (4, 4), 1, out=w)
+                    pl._lwt(w, wv, 0, 2, (0, 1), (4, 4), 1, out=y)
+
+                for _ in range(2):
+                    step()
+                torch.cuda.synchronize(dev)
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+                    step()
+                graph.replay()
+                torch.cuda.synchronize(dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                n = steps if on else 2
+                e0.record()
+                for _ in range(n):
+                    graph.replay()
+                e1.record()
+                torch.cuda.synchronize(dev)
+                ms = e0.elapsed_time(e1) / n
+                res["generic" if on else "general_kernel"] = round(B / ms / 1e6, 3)
+                del graph
+            finally:
+                _lib.set_option("generic_kernels", 1)
+        out[f"wavelet_{wv}"] = res
+    return out
+
+
 def inverse_section(dev, x, steps: int = 10):
     """Inverse + InverseAdjoint of the headline workload (the same kernels
     with the step order and signs of those transforms), timed as a CUDA
@@ -625,7 +674,7 @@ def main() -> int:
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched, autograd and least-squares sections")
     ap.add_argument("--section", choices=["inverse", "cfg1", "batched", "batched_nd", "autograd",
-                                          "lsq"],
+                                          "lsq", "generic"],
                     help="run only this section (one GPU) and print its JSON; for profiling "
                          "its kernels, not a driver line")
     args = ap.parse_args()
@@ -650,7 +699,7 @@ def main() -> int:
             res = inverse_section(dev, xi)
         else:
             fn = {"cfg1": cfg1_section, "batched": batched_section,
-                  "batched_nd": batched_nd_section,
+                  "batched_nd": batched_nd_section, "generic": generic_section,
                   "autograd": autograd_section, "lsq": lsq_section}[args.section]
             res = fn(dev)
         print(json.dumps({"section": args.section, **res}))
@@ -813,7 +862,7 @@ def main() -> int:
                              f"{cores} threads)"}
 
     extras = {"inverse": None, "cfg1_1d_f64": None, "batched": None, "batched_nd": None,
-              "autograd": None, "lsq": None}
+              "autograd": None, "lsq": None, "generic": None}
     if world == 1 and not args.no_extras:
         extras["inverse"] = inverse_section(dev, x)
         extras["cfg1_1d_f64"] = cfg1_section(dev)
@@ -821,6 +870,7 @@ def main() -> int:
         extras["batched_nd"] = batched_nd_section(dev)
         extras["autograd"] = autograd_section(dev)
         extras["lsq"] = lsq_section(dev)
+        extras["generic"] = generic_section(dev)
 
     if world > 1:
         dist.barrier()
@@ -853,6 +903,7 @@ def main() -> int:
             "cfg1_1d_f64": extras["cfg1_1d_f64"],
             "batched": extras["batched"],
             "batched_nd": extras["batched_nd"],
+            "generic_wavelets": extras["generic"],
             "autograd": extras["autograd"],
             "lsq": extras["lsq"],
         }
