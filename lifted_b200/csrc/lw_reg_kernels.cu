@@ -556,10 +556,12 @@ bool col_chain_ok(int wi, int op, int64_t n, int levels, int depth) {
   return compiled_wavelet(wi) && m % (2 * P0) == 0 && m / (2 * P0) <= 16;
 }
 
-// Strided float32 pass on the TMA-staged persistent kernel: whole lines of
-// up to 512 samples, or 512-sample windows with halos on longer lines; the
-// levels beyond the first k run as a strided whole-line launch on the
-// approximation band.  Returns 0 when the pass does not qualify.
+// Strided pass (float32 or float64) on the TMA-staged persistent kernel:
+// whole lines of up to 512 samples (several 3D slices per window when they
+// are short), or 512-sample windows with halos on longer lines; the levels
+// beyond the first k run as further launches on the approximation band
+// (band_pass).  Catalogue wavelets without compiled kernels use the generic
+// instantiations.  Returns 0 when the pass does not qualify.
 template <typename T>
 int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   {
