@@ -69,6 +69,26 @@ bool set_gen_shapes(DevProgram<T>* p, int op) {
   return true;
 }
 
+// Whether, at some level, a step's front and back edge ranges overlap (a
+// band shorter than the taps reaching into it from both sides): there the
+// reference updates the overlapping indices twice (front, then back), which
+// the register kernels, which skip out-of-band taps once, do not reproduce.
+// Bands of n >> (l + 1) pairs (every level's band a whole number of pairs).
+template <typename T>
+bool edges_overlap(const DevProgram<T>& prog, int64_t n, int levels) {
+  for (int l = 0; l < levels; ++l) {
+    const int64_t ny = n >> (l + 1);
+    for (int k = 0; k < prog.nsteps; ++k) {
+      const DevStep<T>& st = prog.st[k];
+      if (st.kind == K_SCALE) continue;
+      const int64_t n1 = st.nf < ny ? (int64_t)st.nf : ny;
+      const int64_t n2 = ny > st.nb ? ny - st.nb : 0;
+      if (n1 > n2) return true;
+    }
+  }
+  return false;
+}
+
 // The host-resolved program must have exactly the compile-time structure.
 template <typename T>
 bool structure_matches(const DevProgram<T>& prog, int wi, int op) {
@@ -283,8 +303,13 @@ int launch_wtile(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) 
   const int p0 = wtile_pairs((int)sizeof(T));
   const int64_t W = 64 * (int64_t)p0;
   const int64_t n = g.n;
-  if (n <= W || n % (2 * p0)) return 0;
   if (a.levels < 1 || a.levels > wtile_levels(a.wi, a.op, (int)sizeof(T))) return 0;
+  // every level's band a whole number of pairs: n a multiple of 2^levels;
+  // lengths that are not multiples of a lane's pairs mask the band's end
+  // (rows up to one window are one window)
+  if (n < 2 || n % ((int64_t)1 << a.levels)) return 0;
+  const bool end_mask = (n % (2 * p0)) != 0;
+  if (!end_mask && n <= W) return 0;  // the warp-per-row kernel takes these
   // halo: the samples k levels corrupt from a window edge, whole lanes
   int64_t need = 0;
   const int lh = cat_level_halo(a.wi, a.op);
@@ -310,8 +335,8 @@ int launch_wtile(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) 
   if (grid > 0x7fffffffLL) return 0;
   const size_t smem = (size_t)warps * (size_t)W * sizeof(T);
   cudaError_t e;
-  if constexpr (sizeof(T) == 4) e = launch_wtile_f32(wk, a.op, p, (int)grid, smem, stream);
-  else e = launch_wtile_f64(wk, a.op, p, (int)grid, smem, stream);
+  if constexpr (sizeof(T) == 4) e = launch_wtile_f32(wk, a.op, end_mask, p, (int)grid, smem, stream);
+  else e = launch_wtile_f64(wk, a.op, end_mask, p, (int)grid, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
   if (stats) stats->launches += 1;
   return 1;
@@ -792,6 +817,7 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
   if (a.levels < 1 || a.levels > MAX_LEVELS) return 0;
   if (!structure_matches(*a.prog, a.wi, a.op)) return 0;
   const LineGeom& g = a.g;
+  if (edges_overlap(*a.prog, g.n, a.levels)) return 0;
   const bool contiguous = (g.sin == 1 && g.sout == 1);
   if (!compiled_wavelet(a.wi)) {
     // the generic instantiations: rows of 512-4096 (float32) or 512-2048

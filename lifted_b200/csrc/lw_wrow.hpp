@@ -38,10 +38,11 @@ template <typename T>
 struct WTileParams;
 int wtile_pairs(int elem_bytes);
 int wtile_levels(int wi, int op, int elem_bytes);
-cudaError_t launch_wtile_f32(int wi, int op, const WTileParams<float>& p, int grid, size_t smem,
-                             cudaStream_t stream);
-cudaError_t launch_wtile_f64(int wi, int op, const WTileParams<double>& p, int grid, size_t smem,
-                             cudaStream_t stream);
+// end_mask: the row length is a multiple of 2^levels but not of 2 * pairs
+cudaError_t launch_wtile_f32(int wi, int op, bool end_mask, const WTileParams<float>& p, int grid,
+                             size_t smem, cudaStream_t stream);
+cudaError_t launch_wtile_f64(int wi, int op, bool end_mask, const WTileParams<double>& p,
+                             int grid, size_t smem, cudaStream_t stream);
 // Whether long contiguous rows may use it (the "row_windows" option).
 bool wtile_enabled();
 // Whether catalogue wavelets without compiled kernels may use the generic

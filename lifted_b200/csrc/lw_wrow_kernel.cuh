@@ -126,10 +126,15 @@ __device__ __forceinline__ void write_run(T* buf, int e, const T (&v)[PA]) {
 // One step over the lane's P pairs; halos by shuffle.  okl / okr: the
 // left / right neighbour lane holds pairs of the same band (whole rows:
 // lane > 0 / lane < the last active lane; windows: also by band position).
+// EM: the band may end inside this lane, after its first `lim` pairs, or
+// inside its right neighbour, after that lane's first `rlim` pairs (windows
+// of rows whose length is not a multiple of the lane's pairs); taps past
+// the end are skipped like taps past the band edge.
 template <typename T, int P, int PA, int KIND, int OFF, int NT, int SUB,
-          int HL, int HR>
+          int HL, int HR, bool EM = false>
 __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
-                                        const DevStep<T>& st, bool okl, bool okr) {
+                                        const DevStep<T>& st, bool okl, bool okr,
+                                        int lim = P, int rlim = P) {
   static_assert(HL <= P && HR <= P, "step reaches past the neighbour lane");
   T xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
 #pragma unroll
@@ -144,27 +149,27 @@ __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
       for (int k = 0; k < NT; ++k) {
         const int idx = i + OFF + k;
         const T v = idx < 0 ? xl[HL + idx] : (idx >= P ? xr[idx - P] : x[idx]);
-        const bool ok = idx < 0 ? okl : (idx >= P ? okr : true);
+        const bool ok = idx < 0 ? okl : (idx >= P ? (okr && (!EM || idx - P < rlim)) : (!EM || idx < lim));
         const T f = fop(SUB, st.c[k], v, yi);
         yi = ok ? f : yi;
       }
     } else if constexpr (KIND == K_REPEAT) {
       int idx = i + OFF;
       T v = idx < 0 ? xl[HL + idx] : (idx >= P ? xr[idx - P] : x[idx]);
-      bool ok = idx < 0 ? okl : (idx >= P ? okr : true);
+      bool ok = idx < 0 ? okl : (idx >= P ? (okr && (!EM || idx - P < rlim)) : (!EM || idx < lim));
       T x0 = ok ? v : T(0);
 #pragma unroll
       for (int k = 1; k < NT; ++k) {
         idx = i + OFF + k;
         v = idx < 0 ? xl[HL + idx] : (idx >= P ? xr[idx - P] : x[idx]);
-        ok = idx < 0 ? okl : (idx >= P ? okr : true);
+        ok = idx < 0 ? okl : (idx >= P ? (okr && (!EM || idx - P < rlim)) : (!EM || idx < lim));
         x0 = ok ? x0 + v : x0;
       }
       yi = fop(SUB, st.c[0], x0, yi);
     } else {
       const int idx = i + OFF;
       const T v = idx < 0 ? xl[HL + idx] : (idx >= P ? xr[idx - P] : x[idx]);
-      const bool ok = idx < 0 ? okl : (idx >= P ? okr : true);
+      const bool ok = idx < 0 ? okl : (idx >= P ? (okr && (!EM || idx - P < rlim)) : (!EM || idx < lim));
       const T f = SUB ? yi - v : yi + v;
       yi = ok ? f : yi;
     }
@@ -175,29 +180,31 @@ __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
 // Generic kernels: the update of one step, dispatched on its shape index
 // (shapes reaching past P pairs are not compiled at this level; the host
 // never runs those levels).
-template <typename T, int OP, int P, int PA, int I>
+template <typename T, int OP, int P, int PA, int I, bool EM = false>
 __device__ __forceinline__ void wgen_update(int shape, T (&s)[PA], T (&d)[PA],
-                                            const DevStep<T>& st, bool okl, bool okr) {
+                                            const DevStep<T>& st, bool okl, bool okr,
+                                            int lim = P, int rlim = P) {
   if constexpr (I < GenTable<OP>::v.n) {
     if (shape == I) {
       constexpr CStep cs = GenTable<OP>::v.s[I];
       if constexpr (cs.left <= P && cs.right <= P) {
         if constexpr (cs.y_is_d)
-          wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, okl,
-                                                                                  okr);
+          wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(
+              d, s, st, okl, okr, lim, rlim);
         else
-          wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, okl,
-                                                                                  okr);
+          wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(
+              s, d, st, okl, okr, lim, rlim);
       }
       return;
     }
-    wgen_update<T, OP, P, PA, I + 1>(shape, s, d, st, okl, okr);
+    wgen_update<T, OP, P, PA, I + 1, EM>(shape, s, d, st, okl, okr, lim, rlim);
   }
 }
 
-template <typename T, int WI, int OP, int K, int P, int PA>
+template <typename T, int WI, int OP, int K, int P, int PA, bool EM = false>
 __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
-                                       const DevProgram<T>& prog, bool okl, bool okr) {
+                                       const DevProgram<T>& prog, bool okl, bool okr,
+                                       int lim = P, int rlim = P) {
   if constexpr (WI == WI_GEN) {
     if constexpr (K == 0) {
       for (int k = 0; k < prog.nsteps; ++k) {
@@ -210,7 +217,7 @@ __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
             d[i] = d[i] * dm;
           }
         } else {
-          wgen_update<T, OP, P, PA, 0>(st.shape, s, d, st, okl, okr);
+          wgen_update<T, OP, P, PA, 0, EM>(st.shape, s, d, st, okl, okr, lim, rlim);
         }
       }
     }
@@ -225,13 +232,13 @@ __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
         d[i] = d[i] * dm;
       }
     } else if constexpr (cs.y_is_d) {
-      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, okl,
-                                                                            okr);
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(d, s, st, okl,
+                                                                                okr, lim, rlim);
     } else {
-      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, okl,
-                                                                            okr);
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(s, d, st, okl,
+                                                                                okr, lim, rlim);
     }
-    wsteps<T, WI, OP, K + 1, P, PA>(s, d, prog, okl, okr);
+    wsteps<T, WI, OP, K + 1, P, PA, EM>(s, d, prog, okl, okr, lim, rlim);
   }
 }
 

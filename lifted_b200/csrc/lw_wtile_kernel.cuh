@@ -95,7 +95,7 @@ __device__ __forceinline__ void drain_band(T* dst, T* buf, int nbl, int b0, int 
   }
 }
 
-template <typename T, int WI, int OP, int P0, int LV>
+template <typename T, int WI, int OP, int P0, int LV, bool EM>
 __device__ __forceinline__ void fwd(T (&s)[P0], T (&d)[P0], T* buf, const DevProgram<T>& prog,
                                     int levels, int lane, int64_t wstart, int64_t n) {
   constexpr int P = P0 >> LV;
@@ -104,8 +104,11 @@ __device__ __forceinline__ void fwd(T (&s)[P0], T (&d)[P0], T* buf, const DevPro
       constexpr int NB = 32 * P;
       const int64_t nbp = n >> (LV + 1);                 // pairs of the row's band
       const int64_t gp0 = (wstart >> (LV + 1)) + (int64_t)lane * P;
-      wrow::wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane > 0 && gp0 > 0,
-                                        lane < 31 && gp0 + P < nbp);
+      const int64_t rem = nbp - gp0;                     // the band ends in this lane
+      const int lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
+      const int rlim = rem - P >= P ? P : (rem - P > 0 ? (int)(rem - P) : 0);  // or the next
+      wrow::wsteps<T, WI, OP, 0, P, P0, EM>(s, d, prog, lane > 0 && gp0 > 0,
+                                            lane < 31 && gp0 + P < nbp, lim, rlim);
       wrow::write_run<T, P, P>(buf, NB + P * lane, d);
       if (LV + 1 == levels) {
         wrow::write_run<T, P, P>(buf, P * lane, s);
@@ -116,12 +119,12 @@ __device__ __forceinline__ void fwd(T (&s)[P0], T (&d)[P0], T* buf, const DevPro
         d[i] = s[2 * i + 1];
         s[i] = s[2 * i];
       }
-      fwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane, wstart, n);
+      fwd<T, WI, OP, P0, LV + 1, EM>(s, d, buf, prog, levels, lane, wstart, n);
     }
   }
 }
 
-template <typename T, int WI, int OP, int P0, int LV>
+template <typename T, int WI, int OP, int P0, int LV, bool EM>
 __device__ __forceinline__ void rev(T (&s)[P0], T (&d)[P0], T* buf, const DevProgram<T>& prog,
                                     int levels, int lane, int64_t wstart, int64_t n) {
   constexpr int P = P0 >> LV;
@@ -131,10 +134,13 @@ __device__ __forceinline__ void rev(T (&s)[P0], T (&d)[P0], T* buf, const DevPro
         constexpr int NB = 32 * P;
         const int64_t nbp = n >> (LV + 1);
         const int64_t gp0 = (wstart >> (LV + 1)) + (int64_t)lane * P;
+        const int64_t rem = nbp - gp0;
+        const int lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
+        const int rlim = rem - P >= P ? P : (rem - P > 0 ? (int)(rem - P) : 0);
         if (LV + 1 == levels) wrow::read_run<T, P, P>(buf, P * lane, s);
         wrow::read_run<T, P, P>(buf, NB + P * lane, d);
-        wrow::wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane > 0 && gp0 > 0,
-                                          lane < 31 && gp0 + P < nbp);
+        wrow::wsteps<T, WI, OP, 0, P, P0, EM>(s, d, prog, lane > 0 && gp0 > 0,
+                                              lane < 31 && gp0 + P < nbp, lim, rlim);
         if constexpr (LV > 0) {
 #pragma unroll
           for (int i = P - 1; i >= 0; --i) {
@@ -144,14 +150,16 @@ __device__ __forceinline__ void rev(T (&s)[P0], T (&d)[P0], T* buf, const DevPro
         }
       }
     }
-    if constexpr (LV > 0) rev<T, WI, OP, P0, LV - 1>(s, d, buf, prog, levels, lane, wstart, n);
+    if constexpr (LV > 0) rev<T, WI, OP, P0, LV - 1, EM>(s, d, buf, prog, levels, lane, wstart, n);
   }
 }
 
 }  // namespace wtile
 
 // 128 threads = four windows, one warp each; no block barriers.
-template <typename T, int WI, int OP, int P0>
+// EM: rows whose length is a multiple of 2^levels but not of 2 * P0 (the
+// band ends inside a lane at some level).
+template <typename T, int WI, int OP, int P0, bool EM>
 __global__ void __launch_bounds__(128)
     wtile_kernel(const __grid_constant__ WTileParams<T> p) {
   constexpr int W = 64 * P0;                  // window samples
@@ -180,15 +188,17 @@ __global__ void __launch_bounds__(128)
 
   T s[P0], d[P0];
   if constexpr (FWD) {
-    // raw window, zeros outside the row (whole 16-byte units either way)
+    // raw window, zeros outside the row (a unit across the row's end is
+    // copied in part and zero-filled)
     const T* src = p.in + bin;
 #pragma unroll 4
     for (int u = lane; u < UNITS; u += 32) {
       const int64_t e = wstart + (int64_t)u * EPU;
       const bool in_row = e >= 0 && e < n;
+      const int bytes = !in_row ? 0 : (e + EPU <= n ? 16 : (int)((n - e) * (int64_t)sizeof(T)));
       const unsigned saddr = (unsigned)__cvta_generic_to_shared(buf + wrow::swz(u, SHA) * EPU);
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr),
-                   "l"(in_row ? src + e : src), "r"(in_row ? 16 : 0)
+                   "l"(in_row ? src + e : src), "r"(bytes)
                    : "memory");
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -201,7 +211,7 @@ __global__ void __launch_bounds__(128)
       d[i] = x[2 * i + 1];
     }
     __syncwarp();
-    wtile::fwd<T, WI, OP, P0, 0>(s, d, buf, p.prog, L, lane, wstart, n);
+    wtile::fwd<T, WI, OP, P0, 0, EM>(s, d, buf, p.prog, L, lane, wstart, n);
     __syncwarp();
     // interiors: d_l at out[n >> l + (t0 >> l) ..], a_L at out[t0 >> L ..]
     T* dst = p.out + bout;
@@ -222,7 +232,7 @@ __global__ void __launch_bounds__(128)
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncwarp();
     constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
-    wtile::rev<T, WI, OP, P0, TOP>(s, d, buf, p.prog, L, lane, wstart, n);
+    wtile::rev<T, WI, OP, P0, TOP, EM>(s, d, buf, p.prog, L, lane, wstart, n);
     __syncwarp();
     T x[2 * P0];
 #pragma unroll
@@ -232,14 +242,18 @@ __global__ void __launch_bounds__(128)
     }
     wrow::write_run<T, 2 * P0, 2 * P0>(buf, 2 * P0 * lane, x);
     __syncwarp();
-    // interior [t0, t1): whole 16-byte units (halo, t0 and t1 are
-    // multiples of 2 * P0)
+    // interior [t0, t1): whole 16-byte units (halo and t0 are multiples of
+    // 2 * P0; a row end inside a unit is stored element by element)
     T* o = p.out + bout + t0;
     const int u0 = (int)(p.halo / EPU);
     const int cnt = (int)((t1 - t0) / EPU);
     for (int j = lane; j < cnt; j += 32)
       *reinterpret_cast<int4*>(o + (int64_t)j * EPU) =
           *reinterpret_cast<const int4*>(buf + wrow::swz(u0 + j, SHA) * EPU);
+    for (int e = cnt * EPU + lane; e < (int)(t1 - t0); e += 32) {
+      const int b = (int)p.halo + e;
+      o[e] = buf[wrow::swz(b / EPU, SHA) * EPU + (b % EPU)];
+    }
   }
 }
 

@@ -92,3 +92,26 @@ def test_all_catalogue_wavelets_long_rows(op, dtype):
                 continue
             g, _ = run(x, w, op, [1], [lv])
             assert np.array_equal(g, o), (w, n, lv)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_rows_of_other_lengths_on_windows(op, dtype):
+    """Row lengths that are multiples of 2^levels but not of a lane's pairs
+    (1000, 1080, 1920, 3000, 12000 samples): the band ends inside a lane, the
+    windowed kernel masks it; compiled and generic wavelets, bit for bit."""
+    rng = np.random.default_rng(120 + op)
+    for w in (2, 4, 100907, 5, 104, 17):
+        width = po.wavelet_width(w)
+        for n in (1000, 1080, 1920, 3000, 12000):
+            tz = (n & -n).bit_length() - 1  # levels that keep every band even
+            mx = po.max_level(width, n) if width > 1 else int(np.log2(n))
+            for lv in sorted({1, min(tz, mx, 3)}):
+                if lv < 1:
+                    continue
+                x = rng.standard_normal((3, n)).astype(dtype)
+                rc, o = po.oracle_sep(x, w, op, 0, [1], [lv])
+                if rc:
+                    continue
+                g, _ = run(x, w, op, [1], [lv])
+                assert np.array_equal(g, o), (w, n, lv)
