@@ -10,9 +10,9 @@
 namespace lw {
 namespace {
 
-template <typename T, int WI, int OP, int V>
+template <typename T, int WI, int OP, int V, bool EM>
 cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_t stream) {
-  auto kern = col_kernel<T, WI, OP, V>;
+  auto kern = col_kernel<T, WI, OP, V, EM>;
   static bool configured[kMaxDevices] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -27,25 +27,25 @@ cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_
   return launch_overlapped(kern, grid, COL_THREADS, smem, stream, p);
 }
 
-template <typename T, int WI, int V>
+template <typename T, int WI, int V, bool EM>
 ColFn<T> by_op(int op) {
   switch (op) {
-    case 0: return launch_one<T, WI, 0, V>;
-    case 1: return launch_one<T, WI, 1, V>;
-    case 2: return launch_one<T, WI, 2, V>;
-    default: return launch_one<T, WI, 3, V>;
+    case 0: return launch_one<T, WI, 0, V, EM>;
+    case 1: return launch_one<T, WI, 1, V, EM>;
+    case 2: return launch_one<T, WI, 2, V, EM>;
+    default: return launch_one<T, WI, 3, V, EM>;
   }
 }
 
-template <typename T, int V>
+template <typename T, int V, bool EM>
 ColFn<T> by_wavelet(int wi, int op) {
   switch (wi) {
-    case 2: return by_op<T, 2, V>(op);
-    case 4: return by_op<T, 4, V>(op);
-    case 33: return by_op<T, 33, V>(op);
-    case WI_GEN: return by_op<T, WI_GEN, V>(op);
+    case 2: return by_op<T, 2, V, EM>(op);
+    case 4: return by_op<T, 4, V, EM>(op);
+    case 33: return by_op<T, 33, V, EM>(op);
+    case WI_GEN: return by_op<T, WI_GEN, V, EM>(op);
     case WI_GENW:
-      if constexpr (sizeof(T) == 4 && V == 1) return by_op<T, WI_GENW, V>(op);
+      if constexpr (sizeof(T) == 4 && V == 1) return by_op<T, WI_GENW, V, EM>(op);
       else return nullptr;
     default: return nullptr;
   }
@@ -53,10 +53,14 @@ ColFn<T> by_wavelet(int wi, int op) {
 
 }  // namespace
 
-ColFn<float> pick_col_f32(int wi, int op, int v) {
-  return v == 2 ? by_wavelet<float, 2>(wi, op) : by_wavelet<float, 1>(wi, op);
+// em: lines whose length is not a multiple of 32 (one line per lane only)
+ColFn<float> pick_col_f32(int wi, int op, int v, bool em) {
+  if (em) return v == 1 ? by_wavelet<float, 1, true>(wi, op) : nullptr;
+  return v == 2 ? by_wavelet<float, 2, false>(wi, op) : by_wavelet<float, 1, false>(wi, op);
 }
-ColFn<double> pick_col_f64(int wi, int op) { return by_wavelet<double, 1>(wi, op); }
+ColFn<double> pick_col_f64(int wi, int op, bool em) {
+  return em ? by_wavelet<double, 1, true>(wi, op) : by_wavelet<double, 1, false>(wi, op);
+}
 
 size_t col_smem_bytes(int hmax, int v, int elem_bytes) {
   return (size_t)COL_ROWS * COL_LANES * v * elem_bytes +

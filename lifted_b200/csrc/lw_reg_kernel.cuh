@@ -276,8 +276,7 @@ struct Ctx {
 template <typename VT>
 __device__ __forceinline__ VT tap(const VT* xl, const bool* vl, const VT* x,
                                   const VT* xr, const bool* vr, int idx, int P,
-                                  int HL, bool& ok) {
-  (void)P;
+                                  int HL, bool& ok, int lim) {
   if (idx < 0) {
     ok = vl[HL + idx];
     return xl[HL + idx];
@@ -286,17 +285,24 @@ __device__ __forceinline__ VT tap(const VT* xl, const bool* vl, const VT* x,
     ok = vr[idx - P];
     return xr[idx - P];
   }
-  ok = true;
+  ok = idx < lim;  // lim = P unless the band ends inside this chunk
   return x[idx];
 }
 
-// y[0..P) updated from x with one step of compile-time shape CS.
+// y[0..P) updated from x with one step of compile-time shape CS.  EM: the
+// band (nb pairs) may end inside a chunk (lines whose length is not a
+// multiple of the chunk); in-chunk taps past the end are skipped.
 template <typename T, typename VT, int P, int PA, int HMAX, int KIND, int OFF,
-          int NT, int SUB, int HL, int HR>
+          int NT, int SUB, int HL, int HR, bool EM = false>
 __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
                                        const DevStep<T>& st, Ctx<T>& c,
                                        int64_t gp0, int64_t nb) {
   static_assert(HL <= P && HR <= P, "step reaches past the neighbour chunk");
+  int lim = P;
+  if constexpr (EM) {
+    const int64_t rem = nb - gp0;
+    lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
+  }
   const int nth = c.nth;
   VT* mb = reinterpret_cast<VT*>(c.mb);
   VT* mb_first = mb + (int64_t)((c.buf * 2 + 0) * HMAX) * nth;
@@ -326,23 +332,23 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
 #pragma unroll
       for (int k = 0; k < NT; ++k) {
         bool ok;
-        const VT v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok);
+        const VT v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok, lim);
         const VT f = vfop(SUB, st.c[k], v, yi);
         yi = ok ? f : yi;
       }
     } else if constexpr (KIND == K_REPEAT) {
       bool ok;
-      VT v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok);
+      VT v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok, lim);
       VT x0 = ok ? v : vzero<VT>();
 #pragma unroll
       for (int k = 1; k < NT; ++k) {
-        v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok);
+        v = tap(xl, vl, x, xr, vr, i + OFF + k, P, HL, ok, lim);
         x0 = ok ? vadd(x0, v) : x0;
       }
       yi = vfop(SUB, st.c[0], x0, yi);
     } else {  // unit
       bool ok;
-      const VT v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok);
+      const VT v = tap(xl, vl, x, xr, vr, i + OFF, P, HL, ok, lim);
       const VT f = SUB ? vsub(yi, v) : vadd(yi, v);
       yi = ok ? f : yi;
     }
@@ -353,7 +359,7 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
 // Generic instantiation: one step's update dispatched on its shape index
 // (shapes wider than P pairs or than the exchange width are not compiled;
 // the host never runs them).  Every thread takes the same branch.
-template <typename T, typename VT, int OP, int P, int PA, int HMAX, int I>
+template <typename T, typename VT, int OP, int P, int PA, int HMAX, int I, bool EM = false>
 __device__ __forceinline__ void gen_update(int shape, VT (&s)[PA], VT (&d)[PA],
                                            const DevStep<T>& st, Ctx<T>& c, int64_t gp0,
                                            int64_t nb) {
@@ -362,20 +368,20 @@ __device__ __forceinline__ void gen_update(int shape, VT (&s)[PA], VT (&d)[PA],
       constexpr CStep cs = GenTable<OP>::v.s[I];
       if constexpr (cs.left <= P && cs.right <= P && cs.left <= HMAX && cs.right <= HMAX) {
         if constexpr (cs.y_is_d)
-          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(
+          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(
               d, s, st, c, gp0, nb);
         else
-          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(
+          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(
               s, d, st, c, gp0, nb);
       }
       return;
     }
-    gen_update<T, VT, OP, P, PA, HMAX, I + 1>(shape, s, d, st, c, gp0, nb);
+    gen_update<T, VT, OP, P, PA, HMAX, I + 1, EM>(shape, s, d, st, c, gp0, nb);
   }
 }
 
 template <typename T, typename VT, int WI, int OP, int K, int P, int PA,
-          int HMAX>
+          int HMAX, bool EM = false>
 __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
                                       int64_t gp0, int64_t nb) {
   if constexpr (is_gen(WI)) {
@@ -391,7 +397,7 @@ __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
             d[i] = vmul(d[i], dm);
           }
         } else {
-          gen_update<T, VT, OP, P, PA, HMAX, 0>(st.shape, s, d, st, c, gp0, nb);
+          gen_update<T, VT, OP, P, PA, HMAX, 0, EM>(st.shape, s, d, st, c, gp0, nb);
         }
       }
     }
@@ -407,12 +413,12 @@ __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
       }
     } else if constexpr (cs.y_is_d) {
       update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
-             cs.right>(d, s, st, c, gp0, nb);
+             cs.right, EM>(d, s, st, c, gp0, nb);
     } else {
       update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
-             cs.right>(s, d, st, c, gp0, nb);
+             cs.right, EM>(s, d, st, c, gp0, nb);
     }
-    steps<T, VT, WI, OP, K + 1, P, PA, HMAX>(s, d, c, gp0, nb);
+    steps<T, VT, WI, OP, K + 1, P, PA, HMAX, EM>(s, d, c, gp0, nb);
   }
 }
 
@@ -445,14 +451,27 @@ __device__ __forceinline__ void store_run(const VT (&v)[PA], Ctx<T>& c,
   for (int i = 0; i < P; ++i) *reinterpret_cast<VT*>(o + i * p.g.sout) = v[i];
 }
 
+// store_run limited to the first `lim` positions (a band ending inside the
+// chunk), one store per position.
+template <typename T, typename VT, int P, int PA>
+__device__ __forceinline__ void store_first(const VT (&v)[PA], Ctx<T>& c, int64_t pos0, int lim) {
+  const RegParams<T>& p = *c.p;
+  T* o = p.out + c.bout + pos0 * p.g.sout;
+#pragma unroll
+  for (int i = 0; i < P; ++i)
+    if (i < lim) *reinterpret_cast<VT*>(o + i * p.g.sout) = v[i];
+}
+
 template <typename T>
 __device__ __forceinline__ bool chunk_stored(const Ctx<T>& c) {
   return c.line_ok && c.e0 >= c.tile_lo && c.e0 < c.tile_hi;
 }
 
 // Forward-stepping register levels (Forward, InverseAdjoint).
+// EM: lines whose length is a multiple of 2^levels but not of the chunk;
+// the band ends inside a chunk, whose stores stop there.
 template <typename T, typename VT, int V, int WI, int OP, int P0, int HMAX,
-          int LV, bool TILE>
+          int LV, bool TILE, bool EM = false>
 __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
                                            Ctx<T>& c) {
   constexpr int P = P0 >> LV;
@@ -460,8 +479,16 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
     if (LV < c.p->nreg) {
       const int64_t nb = c.n >> (LV + 1);
       const int64_t gp0 = c.e0 >> (LV + 1);
-      steps<T, VT, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
-      if (chunk_stored(c)) store_run<T, VT, P, P0>(d, c, nb + gp0);
+      int lim = P;
+      if constexpr (EM) {
+        const int64_t rem = nb - gp0;
+        lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
+      }
+      steps<T, VT, WI, OP, 0, P, P0, HMAX, EM>(s, d, c, gp0, nb);
+      if (chunk_stored(c)) {
+        if constexpr (EM) store_first<T, VT, P, P0>(d, c, nb + gp0, lim);
+        else store_run<T, VT, P, P0>(d, c, nb + gp0);
+      }
       if (LV + 1 == c.p->nreg) {
         // hand the approximation band on
         if (TILE && c.p->nreg < c.p->levels) {
@@ -469,12 +496,18 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
             T* t = c.p->tmp + c.L * c.p->tmp_line;
 #pragma unroll
             for (int i = 0; i < P; ++i)
-              *reinterpret_cast<VT*>(t + (gp0 + i) * c.p->tmp_pos) = s[i];
+              if (!EM || i < lim) *reinterpret_cast<VT*>(t + (gp0 + i) * c.p->tmp_pos) = s[i];
           }
         } else if (TILE) {
-          if (chunk_stored(c)) store_run<T, VT, P, P0>(s, c, gp0);
+          if (chunk_stored(c)) {
+            if constexpr (EM) store_first<T, VT, P, P0>(s, c, gp0, lim);
+            else store_run<T, VT, P, P0>(s, c, gp0);
+          }
         } else if (c.p->nreg == c.p->levels) {
-          if (c.line_ok) store_run<T, VT, P, P0>(s, c, gp0);
+          if (c.line_ok) {
+            if constexpr (EM) store_first<T, VT, P, P0>(s, c, gp0, lim);
+            else store_run<T, VT, P, P0>(s, c, gp0);
+          }
         } else {
 #pragma unroll
           for (int v = 0; v < V; ++v) {
@@ -490,7 +523,7 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
         d[i] = s[2 * i + 1];
         s[i] = s[2 * i];
       }
-      fwd_levels<T, VT, V, WI, OP, P0, HMAX, LV + 1, TILE>(s, d, c);
+      fwd_levels<T, VT, V, WI, OP, P0, HMAX, LV + 1, TILE, EM>(s, d, c);
     }
   }
 }

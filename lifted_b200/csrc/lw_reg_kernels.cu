@@ -569,13 +569,14 @@ bool col_levels_plan(int wi, int op, int64_t n, int levels, int* k_out, int64_t*
 // before the first launch, so no launch is left without its band pass.
 template <typename T>
 bool col_chain_ok(int wi, int op, int64_t n, int levels, int depth) {
-  if (depth > 8 || n % 32) return false;
+  // lines a multiple of 32 long, or of 2^levels (the band ends inside a
+  // chunk: the end-masked instantiation)
+  if (depth > 8 || (n % 32 && n % ((int64_t)1 << levels))) return false;
   int k;
   int64_t tile, halo, ntr;
   if (!col_levels_plan<T>(wi, op, n, levels, &k, &tile, &halo, &ntr)) return false;
   if (levels == k) return true;
   const int64_t m = n >> k;
-  if (m % 32) return false;
   if (col_chain_ok<T>(wi, op, m, levels - k, depth + 1)) return true;
   constexpr int P0 = p0_of<T>();
   return compiled_wavelet(wi) && m % (2 * P0) == 0 && m / (2 * P0) <= 16;
@@ -600,7 +601,10 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (g.nother == 2 && (g.oin[1] <= 0 || ((g.oin[1] * EB) & 15))) return 0;
     if (!aligned16(a.in)) return 0;
     const int64_t n = g.n;
-    if (n % 32) return 0;
+    // lines whose length is a multiple of 2^levels but not of 32: the
+    // end-masked instantiation, one line per lane
+    const bool em = (n % 32) != 0;
+    if (em && n % ((int64_t)1 << a.levels)) return 0;
     const int wi = a.wi, op = a.op;
     // two adjacent lines per lane (packed FP32x2) when the line groups and
     // every line base of the output stay 8-byte aligned
@@ -616,7 +620,9 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // short whole lines of a 3D view: a tile stacks 512/n consecutive outer
     // slices (the staging window stays full)
     int stack = 1;
-    if (col_stacked() && n <= COL_ROWS / 2 && COL_ROWS % n == 0 && g.nother == 2 && nouter >= 2)
+    // (each slice whole chunks: a chunk never straddles two slices)
+    if (col_stacked() && !em && n <= COL_ROWS / 2 && COL_ROWS % n == 0 && g.nother == 2 &&
+        nouter >= 2)
       stack = (int)(COL_ROWS / n);
     const int64_t ngroups = (nouter + stack - 1) / stack;
     // packed lanes only while they still give every SM a tile
@@ -633,8 +639,9 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (wide) v = 1;
     const int wk = wide ? WI_GENW : (gen ? WI_GEN : wi);
     ColFn<T> fn;
-    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v);
-    else fn = pick_col_f64(wk, op);
+    if (em) v = 1;
+    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v, em);
+    else fn = pick_col_f64(wk, op, em);
     if (!fn) return 0;
     const int64_t m = n >> k;
     const bool more = a.levels > k;

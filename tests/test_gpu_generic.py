@@ -115,3 +115,26 @@ def test_rows_of_other_lengths_on_windows(op, dtype):
                     continue
                 g, _ = run(x, w, op, [1], [lv])
                 assert np.array_equal(g, o), (w, n, lv)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_columns_and_images_of_other_lengths(op, dtype):
+    """Strided lines whose length is a multiple of 2^levels but not of 32
+    (whole lines, windows, a chained band, 3D views) and 2D images of such
+    sizes (1080 x 1920, 1000 x 3000): compiled and generic wavelets, bit for
+    bit against the oracle."""
+    rng = np.random.default_rng(130 + op)
+    cases = [((200, 64), [0], [3]), ((1000, 64), [0], [3]), ((1080, 96), [0], [3]),
+             ((1920, 32), [0], [6]), ((3000, 32), [0], [3]), ((1000, 4, 32), [0], [3]),
+             ((16, 8, 64), [1], [1]), ((48, 6, 32), [0, 1], [4, 1]),
+             ((1080, 1920), [0, 1], [3, 3]), ((1000, 3000), [0, 1], [3, 2])]
+    for w in (2, 4, 100907, 5, 104):
+        for shape, axes, lv in cases:
+            x = rng.standard_normal(shape).astype(dtype)
+            rc, o = po.oracle_sep(x, w, op, 0, axes, lv)
+            if rc:
+                continue
+            g, _ = run(x, w, op, axes, lv)
+            assert np.array_equal(g, o), (w, shape, axes, lv)
+    assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
