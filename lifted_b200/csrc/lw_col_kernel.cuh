@@ -54,10 +54,10 @@ struct ColParams {
   CUtensorMap tm_rows[COL_MAXK];
   CUtensorMap tm_tmp;
   RegParams<T> r;       // geometry, program, tile, band buffer, levels
-  int64_t ncols;        // lines along x (multiple of 32*V)
+  int64_t ncols;        // lines along x (the last strip may be partial)
   int64_t nouter;       // z extent (1 for a 2D view)
   int64_t ntr;          // row tiles per strip
-  int64_t ntiles;       // ncols/(32*V) * ntr * nouter
+  int64_t ntiles;       // ceil(ncols/(32*V)) * ntr * nouter
   int32_t rank3;        // tensor maps are 3D
   int32_t a_from_tmp;   // reverse: a_k is in the band buffer (else in `in`)
   int32_t spin_limit;   // mbarrier polls before giving up
@@ -122,7 +122,7 @@ struct TileCoord {
 
 template <typename T, int V>
 __device__ __forceinline__ TileCoord decode(const ColParams<T>& p, int64_t t) {
-  const int64_t nstrips = p.ncols / (COL_LANES * V);
+  const int64_t nstrips = (p.ncols + COL_LANES * V - 1) / (COL_LANES * V);
   const int64_t per_outer = nstrips * p.ntr;
   TileCoord c;
   c.outer = t / per_outer;
@@ -323,9 +323,11 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
     const int64_t outer = tc.outer + zr;
     const int64_t L = outer * p.ncols + tc.col0 + (int64_t)c.j * V;
     c.L = L;
-    // V lines together (ncols % (32 V) == 0); a last group of stacked
-    // slices may run past the outer extent
-    c.line_ok = outer < p.nouter && L < p.r.g.nlines;
+    // V lines together; the last strip of a slice may run past ncols (its
+    // lanes there hold the TMA's zero fill and store nothing), and a last
+    // group of stacked slices past the outer extent
+    c.line_ok = outer < p.nouter && tc.col0 + (int64_t)(c.j + 1) * V <= p.ncols &&
+                L < p.r.g.nlines;
     c.bin = 0;
     c.bout = 0;
     if (c.line_ok) line_base(p.r.g, L, c.bin, c.bout);

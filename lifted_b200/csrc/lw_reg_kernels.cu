@@ -597,7 +597,9 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (g.sin <= 1 || ((g.sin * EB) & 15)) return 0;
     if (!lines_adjacent(g) || g.nother > 2) return 0;
     const int64_t ncols = g.oshape[0];
-    if (ncols % COL_LANES) return 0;
+    // a line count that is not a multiple of 32: the last strip is partial
+    // (band-buffer boxes start at outer * ncols + col0, 16-byte aligned)
+    if (ncols % COL_LANES && (ncols < COL_LANES || ((ncols * EB) & 15))) return 0;
     if (g.nother == 2 && (g.oin[1] <= 0 || ((g.oin[1] * EB) & 15))) return 0;
     if (!aligned16(a.in)) return 0;
     const int64_t n = g.n;
@@ -719,7 +721,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     cp.ncols = ncols;
     cp.nouter = nouter;
     cp.ntr = ntr;
-    cp.ntiles = ncols / (COL_LANES * v) * ntr * ngroups;
+    cp.ntiles = (ncols + COL_LANES * v - 1) / (COL_LANES * v) * ntr * ngroups;
     cp.stack = stack;
     cp.rank3 = rank == 3;
     cp.a_from_tmp = more ? 1 : 0;

@@ -138,3 +138,25 @@ def test_columns_and_images_of_other_lengths(op, dtype):
             g, _ = run(x, w, op, axes, lv)
             assert np.array_equal(g, o), (w, shape, axes, lv)
     assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_columns_of_partial_line_groups(op, dtype):
+    """Strided passes whose line count is not a multiple of 32 (the last
+    group of 32 lines is partial): 2D columns, 3D views with an outer dim,
+    whole lines, windows and a chained band pass (the band buffer's boxes
+    start at outer * lines + first line), bit for bit against the oracle."""
+    rng = np.random.default_rng(170 + op)
+    cases = [((512, 100), [0], [4]), ((1000, 3000), [0], [3]), ((200, 36), [0], [3]),
+             ((64, 6, 36), [0], [2]), ((4, 600, 36), [1], [3]), ((4, 2048, 36), [1], [6]),
+             ((3, 256, 100), [1], [5])]
+    for w in (2, 4, 33, 100907, 5):
+        for shape, axes, lv in cases:
+            x = rng.standard_normal(shape).astype(dtype)
+            rc, o = po.oracle_sep(x, w, op, 0, axes, lv)
+            if rc:
+                continue
+            g, _ = run(x, w, op, axes, lv)
+            assert np.array_equal(g, o), (w, shape, axes, lv)
+    assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
