@@ -311,6 +311,24 @@ def batched_section(dev, plain_sample: int = 300, steps: int = 5):
     cpu = cpu_ref_sample(cpu_once, 2 * 2 * samp * 4)
     if cpu is not None:
         cpu["sample"] += f"; the {len(idx)} sampled signals, one call per signal and transform"
+    # parity of the batch's own outputs on the sampled signals (the plain
+    # calls above overwrote them, so the two launches run once more)
+    pf.run(x, out=y, graph=True)
+    pa.run(y, out=z, graph=True)
+    pf.check()
+    pa.check()
+    yh, zh = y.cpu().numpy(), z.cpu().numpy()
+    worst, exact = 0.0, True
+    for i in idx:
+        o, L = int(offs[i]), int(lengths[i])
+        rc, fy = po.oracle_sep(xh[o:o + L], int(ws[i]), 0, 0, [0], [lv[i]])
+        rc2, fz = po.oracle_sep(fy, int(ws[i]), 2, 0, [0], [lv[i]])
+        for got, want in ((yh[o:o + L], fy), (zh[o:o + L], fz)):
+            if not np.array_equal(got, want):
+                exact = False
+                scale = max(float(np.abs(want).max()), 1e-30)
+                worst = max(worst, float(np.abs(got - want).max()) / scale)
+    parity = "bit-exact" if exact else f"max normwise error {worst:.3e}"
     pf.close()
     pa.close()
     gbs = bytes_step / ms / 1e6
@@ -326,6 +344,9 @@ def batched_section(dev, plain_sample: int = 300, steps: int = 5):
                                          f"({samp} samples), one C ABI call per signal "
                                          f"and transform, wall clock"},
             "speedup_vs_plain": round(gbs / plain_gbs, 1),
+            "parity": parity,
+            "parity_sample": f"the {len(idx)} sampled signals of the batch's own Forward and "
+                             f"ForwardAdjoint outputs against the CPU oracle",
             "cpu_reference": cpu}
 
 

@@ -152,8 +152,14 @@ LIFTED_CAPI int lifted_lwt_sep_program_f64(
  *     loads the library until exit); a line longer than that array can hold
  *     (LIFTED_NOALLOC_SCRATCH_BYTES / 6 float32 elements, about 5.6 million)
  *     is rejected with LIFTED_ETOOLARGE;
- *   - the first call on a device looks up the array's device address, so
- *     make it before any stream capture;
+ *   - the first call on a device looks up the array's device address; with
+ *     lazy module loading (the CUDA default) that is also when the module
+ *     loads and the array's memory is reserved on the device, so make the
+ *     first call before the application takes the GPU's memory and before
+ *     any stream capture (or run with CUDA_MODULE_LOADING=EAGER);
+ *   - in and out must be on the current device (else LIFTED_EINVAL);
+ *   - lifted_set_option settings apply, but the fast kernels are never used
+ *     (they allocate scratch), so this entry point serves the general kernel;
  *   - every call shares the array: calls whose kernels overlap on the GPU
  *     (two streams, two host threads) race and must be serialised. */
 #define LIFTED_NOALLOC_SCRATCH_BYTES (32u << 20)
@@ -219,12 +225,19 @@ LIFTED_CAPI int lifted_lwt_batch_nd_f64(uint32_t op, uint32_t bc, size_t nimages
  *   whole_max    longest band transformed as one whole item in shared
  *                memory (default 4096 float32, 2048 float64)
  *   tile         interior width of a tile item, samples of its band
- *   tile_levels  levels per tile group (Zero boundary only) */
+ *   tile_levels  levels per tile group (Zero boundary only)
+ *   spin_limit   polls of a completion counter before an item that waits
+ *                for another item's band gives up (records LIFTED_ETIMEOUT
+ *                for lifted_batch_check, skips its work and lets its own
+ *                dependents proceed): 0 = default (4 M polls, about a
+ *                second), > 0 = that many, < 0 = none, so every waiting
+ *                item gives up at once (failure-detection tests) */
 typedef struct lifted_batch_tuning {
   uint32_t block;
   uint32_t whole_max;
   uint32_t tile;
   uint32_t tile_levels;
+  int32_t spin_limit;
 } lifted_batch_tuning_t;
 
 typedef struct lifted_batch_info {
@@ -305,6 +318,12 @@ LIFTED_CAPI const char* lifted_last_error(void);
 /* Number of kernel launches this library has issued from the calling
  * process (for instrumentation). */
 LIFTED_CAPI uint64_t lifted_launch_count(void);
+/* Launches of one kernel family since the process started (for tests that
+ * check which kernel served a pass; no counterpart in the reference):
+ * "line" (the exact general kernel), "reg", "wrow", "wrow2", "wtile",
+ * "col" (the TMA-staged strided kernel), "batch", "copy", "blur".  0 for an
+ * unknown name. */
+LIFTED_CAPI uint64_t lifted_kernel_launch_count(const char* family);
 /* Process-wide tuning/testing knobs:
  *   "force_global_scratch" 0/1  keep line buffers in global scratch even
  *                               when a line fits in shared memory

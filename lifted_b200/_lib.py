@@ -82,6 +82,7 @@ class BatchTuning(ctypes.Structure):
         ("whole_max", ctypes.c_uint32),
         ("tile", ctypes.c_uint32),
         ("tile_levels", ctypes.c_uint32),
+        ("spin_limit", ctypes.c_int32),
     ]
 
 
@@ -129,6 +130,7 @@ _SIGS["lifted_wavelet_value"] = (_u32, [_sz])
 _SIGS["lifted_status_string"] = (ctypes.c_char_p, [ctypes.c_int])
 _SIGS["lifted_last_error"] = (ctypes.c_char_p, [])
 _SIGS["lifted_launch_count"] = (ctypes.c_uint64, [])
+_SIGS["lifted_kernel_launch_count"] = (ctypes.c_uint64, [ctypes.c_char_p])
 _SIGS["lifted_set_option"] = (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64])
 _SIGS["lifted_device_check"] = (ctypes.c_int, [_p])
 _SIGS["lifted_lwt_batch_nd_f32"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
@@ -173,6 +175,11 @@ def check(status: int) -> None:
 
 def launch_count() -> int:
     return int(load().lifted_launch_count())
+
+
+def kernel_launches(family: str) -> int:
+    """Launches of one kernel family so far ("line", "col", "wrow2", ...)."""
+    return int(load().lifted_kernel_launch_count(family.encode()))
 
 
 def set_option(name: str, value: int) -> None:

@@ -3,8 +3,10 @@
 
     python -m lifted_b200.build [--force] [-j N]
 
-Objects go to lifted_b200/_build/.  Sources are recompiled when they or any
-header they may include is newer than their object.
+Objects go to $LIFTED_BUILD_DIR, else lifted_b200_build/ under the system's
+temporary directory, outside the source tree (only the linked library sits
+in-tree).  Sources are recompiled when they or any header they may include
+is newer than their object.
 """
 from __future__ import annotations
 
@@ -14,12 +16,14 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
-BUILD = PKG / "_build"
+BUILD = Path(os.environ.get("LIFTED_BUILD_DIR") or
+             Path(tempfile.gettempdir()) / "lifted_b200_build")
 LIB = PKG / "liblifted_b200.so"
 
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
@@ -69,7 +73,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     """Compiles every CUDA/C++ source for sm_100a and links the library."""
     if shutil.which(NVCC) is None and not Path(NVCC).exists():
         raise RuntimeError(f"nvcc not found at {NVCC}")
-    BUILD.mkdir(exist_ok=True)
+    BUILD.mkdir(parents=True, exist_ok=True)
     cu, cpp = _sources()
     hdr = _headers()
     tasks = []

@@ -12,9 +12,11 @@ same constants as the reference's ``static_cast<T>(literal)``
 ``L`` suffix).
 
 Usage: python gen_catalogue.py [path/to/lifted/src] > wavelet_catalogue.inc
-(default source directory: /root/reference/src).  The generated file is
-committed; this script only reruns when the catalogue changes.
+(default: $LIFTED_REFERENCE/src, else the src/ of a checkout named
+"reference" beside this repository).  The generated file is committed; this
+script only reruns when the catalogue changes.
 """
+import os
 import re
 import sys
 from pathlib import Path
@@ -39,7 +41,12 @@ def split_args(args: str):
 
 
 def main() -> None:
-    src = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) > 1:
+        src = Path(sys.argv[1])
+    elif os.environ.get("LIFTED_REFERENCE"):
+        src = Path(os.environ["LIFTED_REFERENCE"]) / "src"
+    else:
+        src = Path(__file__).resolve().parents[3] / "reference" / "src"
     cat = strip_comments((src / "lifted-wavelets.hpp").read_text())
     common = (src / "lifted-common.hpp").read_text()
     wav_block = common[common.index("#define LIFTED_WAVELETS"):]

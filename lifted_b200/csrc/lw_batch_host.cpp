@@ -458,6 +458,7 @@ int plan_create(uint32_t op, uint32_t bc, size_t nsig,
                      "batch tiles need %zu bytes of shared memory (limit %zu): "
                      "lower the tile width or whole_max", plan->smem, kMaxDynSmem);
   plan->block = block;
+  if (tu && tu->spin_limit) plan->spin_limit = tu->spin_limit > 0 ? tu->spin_limit : 0;
   plan->scratch_bytes = (size_t)scratch * sizeof(T);
 
   plan->progs_bytes = dprogs.size() * sizeof(DevProgram<T>);
@@ -564,7 +565,10 @@ int plan_run(lifted_batch_plan* p, const T* in, T* out, cudaStream_t stream,
   bp.buf_elems = p->buf_elems;
   bp.spin_limit = p->spin_limit;
   e = launch_batch(bp, p->grid, p->block, p->smem, stream);
-  if (count) count_launches(1);
+  if (count) {
+    count_launches(1);
+    count_family(KF_BATCH, 1);
+  }
   if (e != cudaSuccess) return set_error(LIFTED_ECUDA, "batch kernel launch: %s", cudaGetErrorString(e));
   if (p->last && !capturing) cudaEventRecord(p->last, stream);
   return LIFTED_OK;
@@ -615,6 +619,7 @@ int plan_graph(lifted_batch_plan* p, const void* in, void* out, cudaStream_t str
   }
   cudaError_t e = cudaGraphLaunch(p->gexec, stream);
   count_launches(1);
+  count_family(KF_BATCH, 1);
   if (e != cudaSuccess) return set_error(LIFTED_ECUDA, "graph launch: %s", cudaGetErrorString(e));
   return LIFTED_OK;
 }

@@ -131,6 +131,7 @@ LIFTED_CAPI int lifted_blur2d_f32(const float* in, float* out, size_t nimg, size
   }
   if (e != cudaSuccess) return set_error(LIFTED_ECUDA, "blur launch: %s", cudaGetErrorString(e));
   count_launches(1);
+  count_family(KF_BLUR, 1);
   return LIFTED_OK;
 }
 

@@ -98,20 +98,21 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int li
   return false;
 }
 
-// TMA load of one box into shared memory (no multicast).
+// TMA load of one box into shared memory (no multicast), with an L2 cache
+// policy.
 __device__ __forceinline__ void tma_box(void* dst, const CUtensorMap* tm, int x, int y,
-                                        int z, bool rank3, uint64_t* bar) {
+                                        int z, bool rank3, uint64_t* bar, uint64_t pol) {
   if (rank3) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-        "l"(tm), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        ".L2::cache_hint [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar)), "l"(pol)
         : "memory");
   } else {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"(tm), "r"(x), "r"(y), "r"(smem_u32(bar))
+        ".L2::cache_hint [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(pol)
         : "memory");
   }
 }
@@ -140,6 +141,7 @@ template <typename T, bool FWD, int V>
 __device__ __forceinline__ void issue(const ColParams<T>& p, int64_t t, T* stage,
                                       uint64_t* bar) {
   constexpr int W = COL_LANES * V;  // elements per staging row
+  const uint64_t pol = l2_load_policy(p.r.l2hint);
   const TileCoord tc = decode<T, V>(p, t);
   const int x = (int)tc.col0, z = (int)tc.outer;
   const bool r3 = p.rank3 != 0;
@@ -149,9 +151,9 @@ __device__ __forceinline__ void issue(const ColParams<T>& p, int64_t t, T* stage
     // stacked: slices z .. z+stack-1 of n rows each, two boxes of half the
     // slices (256 rows each)
     const bool st = p.stack > 1;
-    tma_box(stage, &p.tm_rows[0], x, (int)tc.wstart, z, r3, bar);
+    tma_box(stage, &p.tm_rows[0], x, (int)tc.wstart, z, r3, bar, pol);
     tma_box(stage + 256 * W, &p.tm_rows[0], x, st ? 0 : (int)tc.wstart + 256,
-            st ? z + p.stack / 2 : z, r3, bar);
+            st ? z + p.stack / 2 : z, r3, bar, pol);
   } else {
     // d_l windows at rows m_l + (wstart >> l), l = 1..k, then a_k
     const int k = p.r.nreg;
@@ -159,18 +161,18 @@ __device__ __forceinline__ void issue(const ColParams<T>& p, int64_t t, T* stage
     for (int l = 1; l <= k; ++l) {
       const int64_t ml = p.r.g.n >> l;
       tma_box(stage + (size_t)row * W, &p.tm_rows[l - 1], x, (int)(ml + (tc.wstart >> l)), z,
-              r3, bar);
+              r3, bar, pol);
       row += COL_ROWS >> l;
     }
     if (p.a_from_tmp && p.stack > 1) {
       // band buffer viewed as {lines of a slice, position, slice}
-      tma_box(stage + (size_t)row * W, &p.tm_tmp, x, 0, z, true, bar);
+      tma_box(stage + (size_t)row * W, &p.tm_tmp, x, 0, z, true, bar, pol);
     } else if (p.a_from_tmp) {
       // band buffer: x = line index, y = position
       const int64_t L0 = tc.outer * p.ncols + tc.col0;
-      tma_box(stage + (size_t)row * W, &p.tm_tmp, (int)L0, (int)(tc.wstart >> k), 0, false, bar);
+      tma_box(stage + (size_t)row * W, &p.tm_tmp, (int)L0, (int)(tc.wstart >> k), 0, false, bar, pol);
     } else {
-      tma_box(stage + (size_t)row * W, &p.tm_rows[k - 1], x, (int)(tc.wstart >> k), z, r3, bar);
+      tma_box(stage + (size_t)row * W, &p.tm_rows[k - 1], x, (int)(tc.wstart >> k), z, r3, bar, pol);
     }
   }
 }
@@ -245,8 +247,8 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
 #pragma unroll
             for (int i = 0; i < P; ++i) {
               if (!EM || i < lim) {
-                *reinterpret_cast<VT*>(o + (2 * i) * p.g.sout) = s[i];
-                *reinterpret_cast<VT*>(o + (2 * i + 1) * p.g.sout) = d[i];
+                st_hint(o + (2 * i) * p.g.sout, s[i], c.pol_st);
+                st_hint(o + (2 * i + 1) * p.g.sout, d[i], c.pol_st);
               }
             }
           }
@@ -298,6 +300,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   c.has_l = c.r > 0;
   c.has_r = c.r < COL_CHUNKS - 1;
   c.n = p.r.g.n;
+  c.pol_st = l2_store_policy(p.r.l2hint);
   // stacked tiles: chunk r holds chunk rr of slice zr (its own line, whose
   // band edges mask the taps that would reach the neighbouring slices)
   const int cps = p.stack > 1 ? (int)(c.n / (2 * P0)) : COL_CHUNKS;
@@ -314,8 +317,16 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
     if (t + gridDim.x >= p.ntiles) pdl_trigger();  // the CTA's last tile
     const bool got = col::mbar_wait(bar, parity, p.spin_limit);
     if (!__syncthreads_and(got)) {
+      // Give up on the tile (the host reads the flag), but do not leave
+      // while the tile's copy may still be writing this CTA's shared memory,
+      // which the SM hands to the next CTA once this one exits: the copy
+      // of tile t is the only one in flight here (the next tile's copy is
+      // issued after this wait), so wait for it to land, bounded again but
+      // sixteen times longer.  Only a copy that never completes at all gets
+      // past this second bound.
       if (tid == 0) atomicExch(p.err, 1);
-      col::mbar_wait(bar, parity, p.spin_limit);  // let a late copy land
+      col::mbar_wait(bar, parity, 16 * p.spin_limit);  // the host caps spin_limit at 2^22
+      __syncthreads();
       return;
     }
     parity ^= 1;

@@ -18,6 +18,7 @@
 
 #include "../../include/lifted_capi.h"
 #include "lw_host.hpp"
+#include "lw_cache.cuh"
 #include "lw_launch.hpp"
 #include "lw_reg.hpp"
 
@@ -68,6 +69,9 @@ const CatWavelet* find_wavelet(uint32_t value) {
 
 thread_local std::string g_last_error;
 std::atomic<uint64_t> g_launches{0};
+std::atomic<uint64_t> g_family[KF_COUNT] = {};
+const char* const kFamilyNames[KF_COUNT] = {"line", "reg", "wrow", "wrow2", "wtile",
+                                            "col", "batch", "copy", "blur"};
 std::atomic<int64_t> g_opt_force_global{0};
 std::atomic<int64_t> g_opt_max_global_ctas{296};
 std::atomic<int64_t> g_opt_fast_path{1};
@@ -79,6 +83,7 @@ std::atomic<int64_t> g_opt_wrow_split{1};
 std::atomic<int64_t> g_opt_overlap{1};
 std::atomic<int64_t> g_opt_row_windows{1};
 std::atomic<int64_t> g_opt_generic{1};
+std::atomic<int64_t> g_opt_l2_hints{0};
 
 }  // namespace
 
@@ -94,6 +99,17 @@ int set_error(int status, const char* fmt, ...) {
 
 void clear_error() { g_last_error.clear(); }
 void count_launches(uint64_t n) { g_launches += n; }
+void count_family(int fam, uint64_t n) {
+  if (fam >= 0 && fam < KF_COUNT) g_family[fam] += n;
+}
+uint64_t family_count(int fam) {
+  return fam >= 0 && fam < KF_COUNT ? g_family[fam].load() : 0;
+}
+int family_index(const char* name) {
+  for (int i = 0; name && i < KF_COUNT; ++i)
+    if (!std::strcmp(name, kFamilyNames[i])) return i;
+  return -1;
+}
 
 int catalogue_program(uint32_t wavelet, Program* prog) {
   const CatWavelet* w = find_wavelet(wavelet);
@@ -493,6 +509,7 @@ int run_axis_pass(const Program& prog, int op, int bc, int across,
   p.nlines_per_cta_stride = (int64_t)grid * W;
   cudaError_t e = launch_line(p, grid, block, smem, stream);
   count_launches(1);
+  count_family(KF_LINE, 1);
   if (scratch && !opt.scratch) scratch_free(scratch, stream);
   if (e != cudaSuccess)
     return set_error(LIFTED_ECUDA, "line kernel launch: %s",
@@ -520,6 +537,7 @@ int copy_strided(size_t ndim, const int64_t* shape, const int64_t* sin,
   p.ndim = (int32_t)ndim;
   cudaError_t e = launch_copy(p, stream);
   count_launches(1);
+  count_family(KF_COPY, 1);
   if (e != cudaSuccess)
     return set_error(LIFTED_ECUDA, "copy kernel launch: %s",
                      cudaGetErrorString(e));
@@ -839,6 +857,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_row_windows = value ? 1 : 0;
   } else if (!std::strcmp(name, "generic_kernels")) {
     g_opt_generic = value ? 1 : 0;
+  } else if (!std::strcmp(name, "l2_hints")) {
+    g_opt_l2_hints = value ? 1 : 0;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");
@@ -856,6 +876,9 @@ bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
 bool pdl_enabled() { return g_opt_overlap.load() != 0; }
 bool wtile_enabled() { return g_opt_row_windows.load() != 0; }
 bool generic_enabled() { return g_opt_generic.load() != 0; }
+int l2_hint_code() {
+  return g_opt_l2_hints.load() ? l2_code(L2_FIRST, L2_LAST) : l2_code(L2_NORMAL, L2_NORMAL);
+}
 
 }  // namespace lw
 
@@ -944,6 +967,9 @@ LIFTED_CAPI const char* lifted_status_string(int status) {
 }
 LIFTED_CAPI const char* lifted_last_error(void) { return lw::last_error(); }
 LIFTED_CAPI uint64_t lifted_launch_count(void) { return lw::launch_count(); }
+LIFTED_CAPI uint64_t lifted_kernel_launch_count(const char* family) {
+  return lw::family_count(lw::family_index(family));
+}
 LIFTED_CAPI int lifted_device_check(void* stream) {
   lw::clear_error();
   const int v = lw::check_col_errors((cudaStream_t)stream);

@@ -39,6 +39,18 @@ struct PassOptions {
 int set_error(int status, const char* fmt, ...);
 void clear_error();
 void count_launches(uint64_t n);
+// Launches per kernel family, for tests that check which kernel a pass ran
+// on (lifted_kernel_launch_count).
+enum KernelFamily {
+  KF_LINE, KF_REG, KF_WROW, KF_WROW2, KF_WTILE, KF_COL, KF_BATCH, KF_COPY, KF_BLUR,
+  KF_COUNT
+};
+void count_family(int fam, uint64_t n);
+uint64_t family_count(int fam);
+int family_index(const char* name);
+// L2 priority code (lw_cache.cuh) of the fast kernels' loads and stores:
+// evict_first loads and evict_last stores when the "l2_hints" option is on.
+int l2_hint_code();
 const char* last_error();
 uint64_t launch_count();
 

@@ -13,8 +13,17 @@
 //
 // The array's host-side name is only a stand-in for the device address: the
 // kernel gets the address from cudaGetSymbolAddress, taken once per device
-// with that device current, on the first call on the device.  Make that
-// first call before any stream capture.
+// with that device current, on the first call on the device.  With lazy
+// module loading (the CUDA default since 12.2) that first call is also when
+// the module loads and the array's memory is reserved on the device, so make
+// the first call on each device early: before the host application claims
+// the GPU's memory for its own allocator, and before any stream capture (or
+// set CUDA_MODULE_LOADING=EAGER, which reserves it when the library's
+// kernels load).
+//
+// The options of lifted_set_option apply (the general kernel's CTA count
+// among them), except that the fast kernels are never used: they take their
+// scratch from stream-ordered allocations.
 //
 // Every call shares the array and it keeps the last call's contents.  The
 // kernel writes every scratch element before reading it, so nothing needs
@@ -75,7 +84,24 @@ extern "C" LIFTED_CAPI int lifted_lwt_sep_noalloc_f32(
   void* scratch = nullptr;
   rc = lw::noalloc_scratch(&scratch);
   if (rc) return rc;
-  lw::PassOptions opt;
+  // in and out must live on the current device: the scratch array used is
+  // this device's copy.
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess)
+    return lw::set_error(LIFTED_ECUDA, "cudaGetDevice failed");
+  for (const void* ptr : {(const void*)in, (const void*)out}) {
+    if (!ptr) continue;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+      cudaGetLastError();
+      continue;  // host memory: refused below with LIFTED_EINVAL
+    }
+    if ((at.type == cudaMemoryTypeDevice) && at.device != dev)
+      return lw::set_error(LIFTED_EINVAL,
+                           "pointer %p is on device %d, the current device is %d", ptr,
+                           at.device, dev);
+  }
+  lw::PassOptions opt = lw::default_options();
   opt.no_alloc = true;
   opt.fast_path = false;
   opt.scratch = scratch;

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include "lw_host.hpp"
 #include "lw_types.hpp"
 
 namespace lw {
@@ -23,6 +24,12 @@ struct RegPassArgs {
 struct RegStats {
   int launches = 0;
 };
+
+// One launch of kernel family `fam` (KernelFamily, lw_host.hpp).
+inline void counted(RegStats* stats, int fam) {
+  if (stats) stats->launches += 1;
+  count_family(fam, 1);
+}
 
 // Runs one axis pass on the register path when it applies.  Returns 1 when
 // launched, 0 when the pass is not eligible (the caller falls back to the

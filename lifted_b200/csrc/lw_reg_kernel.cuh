@@ -34,6 +34,7 @@
 
 #include <cstdint>
 
+#include "lw_cache.cuh"
 #include "lw_line_kernel.cuh"
 #include "lw_types.hpp"
 
@@ -189,7 +190,7 @@ struct RegParams {
   int32_t vec;            // contiguous unit-stride rows 16-byte aligned
   int32_t coarse_pitch;   // shared coarse buffer: elements per line (A)
   int32_t coarse_pitch_b; // and of its split buffer (B)
-  int32_t pad_;
+  int32_t l2hint;         // L2 priorities of loads and stores (lw_cache.cuh)
   DevProgram<T> prog;
 };
 
@@ -271,6 +272,7 @@ struct Ctx {
   bool has_l, has_r, line_ok;
   int64_t L, bin, bout, n, e0, tile_lo, tile_hi;
   int buf;
+  uint64_t pol_st;  // L2 policy of the band stores
 };
 
 template <typename VT>
@@ -437,10 +439,9 @@ __device__ __forceinline__ void store_run(const VT (&v)[PA], Ctx<T>& c,
 #pragma unroll
         for (int i = 0; i < P; i += VW) {
           if constexpr (sizeof(T) == 4) {
-            *reinterpret_cast<float4*>(o + i) =
-                make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+            st_hint(o + i, make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]), c.pol_st);
           } else {
-            *reinterpret_cast<double2*>(o + i) = make_double2(v[i], v[i + 1]);
+            st_hint(o + i, make_double2(v[i], v[i + 1]), c.pol_st);
           }
         }
         return;
@@ -448,7 +449,7 @@ __device__ __forceinline__ void store_run(const VT (&v)[PA], Ctx<T>& c,
     }
   }
 #pragma unroll
-  for (int i = 0; i < P; ++i) *reinterpret_cast<VT*>(o + i * p.g.sout) = v[i];
+  for (int i = 0; i < P; ++i) st_hint(o + i * p.g.sout, v[i], c.pol_st);
 }
 
 // store_run limited to the first `lim` positions (a band ending inside the
@@ -459,7 +460,7 @@ __device__ __forceinline__ void store_first(const VT (&v)[PA], Ctx<T>& c, int64_
   T* o = p.out + c.bout + pos0 * p.g.sout;
 #pragma unroll
   for (int i = 0; i < P; ++i)
-    if (i < lim) *reinterpret_cast<VT*>(o + i * p.g.sout) = v[i];
+    if (i < lim) st_hint(o + i * p.g.sout, v[i], c.pol_st);
 }
 
 template <typename T>
@@ -496,7 +497,7 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
             T* t = c.p->tmp + c.L * c.p->tmp_line;
 #pragma unroll
             for (int i = 0; i < P; ++i)
-              if (!EM || i < lim) *reinterpret_cast<VT*>(t + (gp0 + i) * c.p->tmp_pos) = s[i];
+              if (!EM || i < lim) st_hint(t + (gp0 + i) * c.p->tmp_pos, s[i], c.pol_st);
           }
         } else if (TILE) {
           if (chunk_stored(c)) {
@@ -587,19 +588,19 @@ __device__ __forceinline__ void rev_levels(VT (&s)[P0], VT (&d)[P0],
 #pragma unroll
               for (int i = 0; i < P; i += VW / 2) {
                 if constexpr (sizeof(T) == 4) {
-                  *reinterpret_cast<float4*>(o + 2 * i) =
-                      make_float4(vlane(s[i], 0), vlane(d[i], 0),
-                                  vlane(s[i + 1], 0), vlane(d[i + 1], 0));
+                  st_hint(o + 2 * i,
+                          make_float4(vlane(s[i], 0), vlane(d[i], 0), vlane(s[i + 1], 0),
+                                      vlane(d[i + 1], 0)),
+                          c.pol_st);
                 } else {
-                  *reinterpret_cast<double2*>(o + 2 * i) =
-                      make_double2(vlane(s[i], 0), vlane(d[i], 0));
+                  st_hint(o + 2 * i, make_double2(vlane(s[i], 0), vlane(d[i], 0)), c.pol_st);
                 }
               }
             } else {
 #pragma unroll
               for (int i = 0; i < P; ++i) {
-                *reinterpret_cast<VT*>(o + (2 * i) * p.g.sout) = s[i];
-                *reinterpret_cast<VT*>(o + (2 * i + 1) * p.g.sout) = d[i];
+                st_hint(o + (2 * i) * p.g.sout, s[i], c.pol_st);
+                st_hint(o + (2 * i + 1) * p.g.sout, d[i], c.pol_st);
               }
             }
           }
@@ -667,6 +668,7 @@ __global__ void __launch_bounds__(512)
   c.has_l = c.r > 0;
   c.has_r = c.r < p.tpl - 1;
   c.buf = 0;
+  c.pol_st = l2_store_policy(p.l2hint);
   int64_t tile_idx = 0, group = blockIdx.x;
   if (TILE) {
     tile_idx = blockIdx.x % p.ntiles;

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include <cuda.h>
 
@@ -200,6 +201,7 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   if (smem > kMaxDynSmem) return 0;
   RegParams<T> p;
   std::memset(&p, 0, sizeof(p));
+  p.l2hint = l2_hint_code();
   p.in = in;
   p.out = out;
   p.g = g;
@@ -217,7 +219,7 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   if (!fn) return 0;
   cudaError_t e = fn(p, (int)groups, block, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
-  if (stats) stats->launches += 1;
+  counted(stats, KF_REG);
   return 1;
 }
 
@@ -240,6 +242,7 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       p.out = a.out;
       p.g = g;
       p.levels = a.levels;
+      p.l2hint = l2_hint_code();
       p.prog = *a.prog;
       const size_t smem = (size_t)4 * (size_t)g.n * sizeof(T);
       const int64_t grid = std::min<int64_t>((g.nlines + 1) / 2,
@@ -247,7 +250,7 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       if (grid <= 0x7fffffffLL) {
         cudaError_t e = launch_wrow2_f32(a.wi, a.op, (int)q0, p, (int)grid, smem, stream);
         if (e != cudaSuccess) return -(int)e - 1000;
-        if (stats) stats->launches += 1;
+        counted(stats, KF_WROW2);
         return 1;
       }
     }
@@ -289,7 +292,7 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   else
     e = launch_wrow_f64(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
-  if (stats) stats->launches += 1;
+  counted(stats, KF_WROW);
   return 1;
 }
 
@@ -338,7 +341,7 @@ int launch_wtile(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) 
   if constexpr (sizeof(T) == 4) e = launch_wtile_f32(wk, a.op, end_mask, p, (int)grid, smem, stream);
   else e = launch_wtile_f64(wk, a.op, end_mask, p, (int)grid, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
-  if (stats) stats->launches += 1;
+  counted(stats, KF_WTILE);
   return 1;
 }
 
@@ -397,6 +400,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
 
   RegParams<T> p;
   std::memset(&p, 0, sizeof(p));
+  p.l2hint = l2_hint_code();
   p.g = g;
   p.tmp = tmp;
   p.tmp_line = 1;          // tmp is [position][line]: lines adjacent
@@ -437,7 +441,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   if (fwd) {
     e = tfn(p, (int)(groups * ntiles), block, smem, stream);
     if (e != cudaSuccess) rc = -(int)e - 1000;
-    else if (stats) stats->launches += 1;
+    else counted(stats, KF_REG);
     if (rc == 1 && more) {
       // levels k+1..: tmp -> the first m positions of every output line
       LineGeom g2 = gt;
@@ -460,7 +464,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
     if (rc == 1) {
       e = tfn(p, (int)(groups * ntiles), block, smem, stream);
       if (e != cudaSuccess) rc = -(int)e - 1000;
-      else if (stats) stats->launches += 1;
+      else counted(stats, KF_REG);
     }
   }
   if (tmp) scratch_free(tmp, stream);
@@ -470,8 +474,10 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
 // Device word the TMA-staged kernel sets when a staging wait gives up.
 int32_t* col_error_flag() {
   static int32_t* flag[kMaxDevices] = {};
+  static std::mutex mu;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
   if (!flag[dev]) {
     if (cudaMalloc((void**)&flag[dev], sizeof(int32_t)) != cudaSuccess) {
       cudaGetLastError();
@@ -700,6 +706,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       return 0;
     }
     RegParams<T>& r = cp.r;
+    r.l2hint = l2_hint_code();
     r.in = a.in;
     r.out = a.out;
     r.tmp = tmp;
@@ -769,7 +776,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (rc == 1) {
       e = fn(cp, grid, smem, stream);
       if (e != cudaSuccess) rc = -(int)e - 1000;
-      else if (stats) stats->launches += 1;
+      else counted(stats, KF_COL);
     }
     if (rc == 1 && fwd && more) {
       LineGeom g2 = gt;

@@ -16,6 +16,7 @@
 
 #include <cstdint>
 
+#include "lw_cache.cuh"
 #include "lw_wrow_kernel.cuh"
 
 namespace lw {
@@ -214,6 +215,8 @@ __global__ void __launch_bounds__(128)
   constexpr int SHA = wrow::swz_shift_bytes(2 * P0 * 4);
   const int g = half * 32 + lane;
   const int64_t step = (int64_t)gridDim.x * 2;
+  const uint64_t pol_ld = l2_load_policy(p.l2hint);
+  const uint64_t pol_st = l2_store_policy(p.l2hint);
 
   auto load = [&](int64_t row, float* buf) {
     int64_t bin, bout;
@@ -223,9 +226,7 @@ __global__ void __launch_bounds__(128)
     for (int u = t64; u < UNITS; u += 64) {
       const int sh = FWD ? SHA : wrow2::banded_shift(u, nbl);
       const unsigned saddr = (unsigned)__cvta_generic_to_shared(buf + wrow::swz(u, sh) * 4);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr),
-                   "l"(src + (int64_t)u * 4)
-                   : "memory");
+      cp_async16_hint(saddr, src + (int64_t)u * 4, pol_ld);
     }
   };
 
@@ -273,8 +274,8 @@ __global__ void __launch_bounds__(128)
 #pragma unroll 4
     for (int u = t64; u < UNITS; u += 64) {
       const int sh = FWD ? wrow2::banded_shift(u, nbl) : SHA;
-      *reinterpret_cast<float4*>(dst + (int64_t)u * 4) =
-          *reinterpret_cast<const float4*>(buf + wrow::swz(u, sh) * 4);
+      st_hint(dst + (int64_t)u * 4, *reinterpret_cast<const float4*>(buf + wrow::swz(u, sh) * 4),
+              pol_st);
     }
     wrow2::row_sync(sm.bar_id);  // buffer drained before a later copy refills it
     cur ^= 1;

@@ -36,6 +36,8 @@ struct WRowParams {
   int32_t levels;      // levels of the pass
   int32_t reg_levels;  // generic instantiation: levels in registers (the
                        // rest on compacted lanes); unused otherwise
+  int32_t l2hint;      // two-warp kernel: L2 priorities (lw_cache.cuh)
+  int32_t pad_;
   DevProgram<T> prog;
 };
 

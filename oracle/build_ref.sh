@@ -9,11 +9,13 @@
 #   oracle/_ref/liblifted_ref_avx2.so     32-byte vectors, x86-64-v3
 #   oracle/_ref/liblifted_ref_avx512.so   64-byte vectors, x86-64-v4
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
-# Skips quietly (exit 0) when the reference tree is absent.
+# Usage: oracle/build_ref.sh [reference_root]
+# The reference checkout is the argument, else $LIFTED_REFERENCE, else a
+# checkout named "reference" beside this repository.  Skips quietly (exit 0)
+# when the reference tree is absent.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-${LIFTED_REFERENCE:-/root/reference}}"
+REF="${1:-${LIFTED_REFERENCE:-$HERE/../../reference}}"
 SRC="$REF/src"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC/lifted.hpp" ]; then
@@ -28,9 +30,11 @@ COMMON=(-std=c++20 -O3 -fPIC -DLIFTED_PTHREADS -DNDEBUG
         -I "$HERE/hwy_shim" -I "$SRC" -w)
 REF_TUS=(lifted-float.cpp lifted-double.cpp lifted-sep-float.cpp lifted-sep-double.cpp)
 
+# objects outside the tree (only the linked libraries sit in oracle/_ref)
+OBJ="${LIFTED_BUILD_DIR:-${TMPDIR:-/tmp}/lifted_b200_build}/ref"
 build_variant() {
   local name="$1" bytes="$2" arch="$3"
-  local dir="$OUT/obj_$name"
+  local dir="$OBJ/obj_$name"
   mkdir -p "$dir"
   local objs=()
   local pids=()

@@ -117,3 +117,36 @@ def test_autotuner_records_a_choice_that_plans_use(tmp_path):
     assert np.array_equal(got, oracle_batch(x, lengths, ws, lv, 0, 0))
     plan.close()
     bt.tune_clear()
+
+
+def test_waits_that_run_out_report_timeout_and_leave_the_context_usable():
+    """Failure detection without a GPU fault: with a spin limit of no polls,
+    every item that waits for another item's band gives up at once; the
+    kernel records the first such item, skips its work, lets its own
+    dependents proceed and returns, and lifted_batch_check reports
+    LIFTED_ETIMEOUT naming a waiting item.  The next run of a plan with the
+    default limit is exact again."""
+    import re
+
+    from lifted_b200.batch import ITEM_FIELDS
+
+    lengths, ws, lv, x = make_batch(240, 40, 6000, np.float32, levels_mode="max")
+    tuning = {"whole_max": 256, "tile": 128, "tile_levels": 1, "spin_limit": -1}
+    plan = BatchPlan(lengths, ws, lv, op=0, dtype="float32", tuning=tuning)
+    items = plan.items()
+    wait_col = ITEM_FIELDS.index("wait_ctr")
+    waiting = set(np.flatnonzero(items[:, wait_col] >= 0).tolist())
+    assert waiting, "the plan has no dependent items"
+    xt = torch.from_numpy(x).cuda()
+    plan.run(xt)
+    lib = _lib.load()
+    rc = lib.lifted_batch_check(plan._plan, torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.ETIMEOUT
+    m = re.search(r"batch item (\d+)", lib.lifted_last_error().decode())
+    assert m and int(m.group(1)) in waiting
+    plan.close()
+    good = BatchPlan(lengths, ws, lv, op=0, dtype="float32",
+                     tuning={"whole_max": 256, "tile": 128, "tile_levels": 1})
+    got = run_plan(good, x)
+    assert np.array_equal(got, oracle_batch(x, lengths, ws, lv, 0, 0))
+    good.close()

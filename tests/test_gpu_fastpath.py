@@ -40,8 +40,8 @@ def run(x, w, tf, bc, axes, levels, fast=True):
 def test_rows_whole_line(dtype):
     rng = np.random.default_rng(21)
     for w in WAVELETS:
-        for n in (32, 64, 256, 1024, 2048, 4096):
-            for lv in (1, 2, 3, 5, 6, 9):
+        for n in (32, 64, 256, 512, 1024, 2048, 4096):
+            for lv in (1, 2, 3, 4, 5, 6, 9):
                 x = rng.standard_normal((3, n)).astype(dtype)
                 for tf in range(4):
                     rc, o = po.oracle_sep(x, w, tf, 0, [1], [lv])
