@@ -351,11 +351,14 @@ def batched_section(dev, plain_sample: int = 300, steps: int = 5):
 
 
 def batched_nd_section(dev, steps: int = 10):
-    """Batched nD images of differing shapes: 48 float32 images (16 of
-    512^2, 16 of 256 x 1024, 8 of 1024^2, 8 of 384 x 640; N(0,1), seed
-    1006), CDF 9/7, 4 levels on both axes, Forward + ForwardAdjoint, each
-    transform one lifted_lwt_batch_nd_f32 call (graph replay), against one
-    separable call per image (the reference's loop of lifted::lwt calls)."""
+    """Batched nD images of differing shapes, CDF 9/7, 4 levels on both axes,
+    Forward + ForwardAdjoint, each transform one lifted_lwt_batch_nd_f32
+    call (graph replay), on two batches of float32 N(0,1) images (seed
+    1006): four shapes (16 of 512^2, 16 of 256 x 1024, 8 of 1024^2, 8 of
+    384 x 640) and 48 distinct shapes (sides U[128, 1024), seed 1008).  Each
+    batch runs as one persistent launch of line items and as one separable
+    call per group of identically shaped images; beside them one separable
+    call per image (the reference's loop of lifted::lwt calls)."""
     import ctypes
 
     import torch
@@ -363,61 +366,87 @@ def batched_nd_section(dev, steps: int = 10):
     from lifted_b200 import pylifted as pl
     from lifted_b200.batch import image_table
 
-    shapes = [(512, 512)] * 16 + [(256, 1024)] * 16 + [(1024, 1024)] * 8 + [(384, 640)] * 8
-    sizes = [a * b for a, b in shapes]
-    total = sum(sizes)
-    g = torch.Generator(device=dev).manual_seed(1006)
-    x = torch.randn(total, device=dev, generator=g)
-    w = torch.empty_like(x)
-    y = torch.empty_like(x)
-    tab, n = image_table(shapes, "cdf9.7", 4)
+    rng = np.random.default_rng(1008)
+    distinct = []
+    while len(distinct) < 48:
+        shp = (int(rng.integers(128, 1024)), int(rng.integers(128, 1024)))
+        if shp not in distinct:
+            distinct.append(shp)
+    four = [(512, 512)] * 16 + [(256, 1024)] * 16 + [(1024, 1024)] * 8 + [(384, 640)] * 8
     lib = _lib.load()
 
-    def step():
-        s = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(lib.lifted_lwt_batch_nd_f32(0, 0, n, ctypes.byref(tab), x.data_ptr(),
-                                               w.data_ptr(), s))
-        _lib.check(lib.lifted_lwt_batch_nd_f32(2, 0, n, ctypes.byref(tab), w.data_ptr(),
-                                               y.data_ptr(), s))
+    def measure(shapes):
+        sizes = [a * b for a, b in shapes]
+        total = sum(sizes)
+        g = torch.Generator(device=dev).manual_seed(1006)
+        x = torch.randn(total, device=dev, generator=g)
+        w = torch.empty_like(x)
+        y = torch.empty_like(x)
+        tab, n = image_table(shapes, "cdf9.7", 4)
+        B = 2 * 2 * total * 4
+        res = {"images": len(shapes), "distinct_shapes": len(set(shapes)),
+               "algorithmic_bytes_per_step": B}
 
-    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
-    views = [(x[o:o + sz].view(shp), w[o:o + sz].view(shp), y[o:o + sz].view(shp))
-             for o, sz, shp in zip(offs, sizes, shapes)]
+        def step():
+            s = torch.cuda.current_stream(dev).cuda_stream
+            _lib.check(lib.lifted_lwt_batch_nd_f32(0, 0, n, ctypes.byref(tab), x.data_ptr(),
+                                                   w.data_ptr(), s))
+            _lib.check(lib.lifted_lwt_batch_nd_f32(2, 0, n, ctypes.byref(tab), w.data_ptr(),
+                                                   y.data_ptr(), s))
 
-    def plain():
-        for xi, wi, yi in views:
-            pl._lwt(xi, 100907, 0, 0, (0, 1), (4, 4), 1, out=wi)
-            pl._lwt(wi, 100907, 0, 2, (0, 1), (4, 4), 1, out=yi)
+        for mode, name in ((1, "persistent"), (2, "grouped")):
+            _lib.set_option("batch_nd_mode", mode)
+            try:
+                for _ in range(3):
+                    step()
+                torch.cuda.synchronize(dev)
+                l0 = _lib.launch_count()
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+                    step()
+                launches = _lib.launch_count() - l0
+                graph.replay()
+                torch.cuda.synchronize(dev)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(steps):
+                    graph.replay()
+                e1.record()
+                torch.cuda.synchronize(dev)
+                ms = e0.elapsed_time(e1) / steps
+                del graph
+            finally:
+                _lib.set_option("batch_nd_mode", 0)
+            res[name] = {"value": round(B / ms / 1e6, 3), "unit": "GB/s",
+                         "ms_per_step": round(ms, 4), "launches_per_step": launches,
+                         "cuda_graph": True}
+        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+        views = [(x[o:o + sz].view(shp), w[o:o + sz].view(shp), y[o:o + sz].view(shp))
+                 for o, sz, shp in zip(offs, sizes, shapes)]
 
-    for _ in range(3):
-        step()
+        def plain():
+            for xi, wi, yi in views:
+                pl._lwt(xi, 100907, 0, 0, (0, 1), (4, 4), 1, out=wi)
+                pl._lwt(wi, 100907, 0, 2, (0, 1), (4, 4), 1, out=yi)
+
         plain()
-    torch.cuda.synchronize(dev)
-    graph = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(graph, capture_error_mode="thread_local"):
-        step()
-    graph.replay()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        graph.replay()
-    e1.record()
-    torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1) / steps
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        plain()
-    torch.cuda.synchronize(dev)
-    ms_plain = (time.perf_counter() - t0) * 1e3 / steps
-    B = 2 * 2 * total * 4
-    return {"workload": "48 float32 images (16 x 512^2, 16 x 256x1024, 8 x 1024^2, 8 x "
-                        "384x640), CDF 9/7 4 levels on both axes, Forward + ForwardAdjoint",
-            "value": round(B / ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(ms, 4),
-            "cuda_graph": True,
-            "plain_per_image": {"value": round(B / ms_plain / 1e6, 3), "unit": "GB/s",
-                                "ms_per_step": round(ms_plain, 4),
-                                "sample": "one separable call per image and transform, wall clock"}}
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            plain()
+        torch.cuda.synchronize(dev)
+        ms_plain = (time.perf_counter() - t0) * 1e3 / steps
+        res["plain_per_image"] = {"value": round(B / ms_plain / 1e6, 3), "unit": "GB/s",
+                                  "ms_per_step": round(ms_plain, 4),
+                                  "sample": "one separable call per image and transform, "
+                                            "wall clock"}
+        return res
+
+    return {"workload": "float32 images, CDF 9/7 4 levels on both axes, Forward + "
+                        "ForwardAdjoint, one lifted_lwt_batch_nd_f32 call per transform",
+            "four_shapes": measure(four),
+            "all_distinct_shapes": measure(distinct)}
 
 
 def generic_section(dev, steps: int = 10):

@@ -262,6 +262,26 @@ LIFTED_CAPI int lifted_batch_plan_create_f64(uint32_t op, uint32_t bc, size_t ns
                                              const lifted_signal_t* signals,
                                              const lifted_batch_tuning_t* tuning,
                                              lifted_batch_plan_t** plan);
+/* A reusable plan of a batch of nD images (the lifted_image_t table that
+ * lifted_lwt_batch_nd_* takes; no counterpart in the reference, whose batch
+ * is a loop of lwt calls, src/pylifted/_wavelets.pyx:185-264): one
+ * persistent launch per run; every (image, axis) pass is cut into line
+ * items of whole lines on the device queue, and the items of an image's
+ * later axes wait (bounded) on a completion counter of its earlier axes.
+ * Run, replay, check, inspect and destroy it with the lifted_batch_* calls.
+ * in == out is allowed when every image's input offset equals its output
+ * offset or its input meets no output.  Tuning: whole_max sets the shared
+ * memory per CTA (1.5 * whole_max elements; longer lines work in a global
+ * slot per CTA), block the CTA size, spin_limit as below; tile and
+ * tile_levels are unused. */
+LIFTED_CAPI int lifted_batch_plan_create_nd_f32(uint32_t op, uint32_t bc, size_t nimages,
+                                                const lifted_image_t* images,
+                                                const lifted_batch_tuning_t* tuning,
+                                                lifted_batch_plan_t** plan);
+LIFTED_CAPI int lifted_batch_plan_create_nd_f64(uint32_t op, uint32_t bc, size_t nimages,
+                                                const lifted_image_t* images,
+                                                const lifted_batch_tuning_t* tuning,
+                                                lifted_batch_plan_t** plan);
 /* Enqueues one run on `stream` (a memset of the queue counters and one
  * kernel launch; stream-ordered, no synchronisation, may be captured into a
  * CUDA graph).  Runs of one plan must not overlap on the GPU. */
@@ -278,10 +298,15 @@ LIFTED_CAPI int lifted_batch_plan_info(const lifted_batch_plan_t* plan,
                                        lifted_batch_info_t* info);
 /* Fields of work item `index` in queue order: kind, program, signal, lev0,
  * nlev, src_sel, dst_sel, wait_ctr, wait_target, done_ctr, n0, in_off,
- * out_off, src_off, dst_off, t0, t1, halo, gbuf, phase (for tests and
+ * out_off, src_off, dst_off, t0, t1, halo, gbuf, phase, geo (for tests and
  * diagnostics). */
 LIFTED_CAPI int lifted_batch_plan_item(const lifted_batch_plan_t* plan, size_t index,
                                        int64_t* fields, size_t nfields);
+/* Axis-pass geometry `index` of a plan of nD images (the `geo` field of its
+ * line items): line length, element stride along the axis, the other three
+ * dims fastest first (1 where absent) and their element strides. */
+LIFTED_CAPI int lifted_batch_plan_geo(const lifted_batch_plan_t* plan, size_t index,
+                                      int64_t* fields, size_t nfields);
 LIFTED_CAPI void lifted_batch_plan_destroy(lifted_batch_plan_t* plan);
 /* One-shot: plan, run, check, destroy (synchronous). */
 LIFTED_CAPI int lifted_lwt_batch_f32(uint32_t op, uint32_t bc, size_t nsignals,
@@ -349,7 +374,18 @@ LIFTED_CAPI uint64_t lifted_kernel_launch_count(const char* family);
  *                               transform kernel in a stream is scheduled
  *                               while the one before it drains, and waits
  *                               in hardware for its results (launches
- *                               recorded by stream capture never use it) */
+ *                               recorded by stream capture never use it)
+ *   "l2_hints"             0/1  fast kernels read with L2 evict_first and
+ *                               write with evict_last (per-instruction
+ *                               cache policies; off: measured no gain)
+ *   "col_row_order"        0/1  the TMA-staged strided kernel takes its
+ *                               tiles row tile by row tile (neighbouring
+ *                               CTAs read neighbouring strips of the same
+ *                               rows; else strip by strip)
+ *   "batch_nd_mode"        0..2 batches of nD images: 0 automatic, 1 one
+ *                               persistent launch of line items, 2 one
+ *                               separable call per group of identically
+ *                               shaped, packed images */
 LIFTED_CAPI int lifted_set_option(const char* name, int64_t value);
 /* Synchronises `stream` and reports LIFTED_ETIMEOUT if a kernel of this
  * library gave up a bounded device-side wait since the last check (the

@@ -116,6 +116,7 @@ _SIGS["lifted_batch_run_graph"] = (ctypes.c_int, [_p, _p, _p, _p])
 _SIGS["lifted_batch_check"] = (ctypes.c_int, [_p, _p])
 _SIGS["lifted_batch_plan_info"] = (ctypes.c_int, [_p, _p])
 _SIGS["lifted_batch_plan_item"] = (ctypes.c_int, [_p, _sz, _p, _sz])
+_SIGS["lifted_batch_plan_geo"] = (ctypes.c_int, [_p, _sz, _p, _sz])
 _SIGS["lifted_batch_plan_destroy"] = (None, [_p])
 _SIGS["lifted_lwt_batch_f32"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
 _SIGS["lifted_lwt_batch_f64"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
@@ -133,6 +134,8 @@ _SIGS["lifted_launch_count"] = (ctypes.c_uint64, [])
 _SIGS["lifted_kernel_launch_count"] = (ctypes.c_uint64, [ctypes.c_char_p])
 _SIGS["lifted_set_option"] = (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64])
 _SIGS["lifted_device_check"] = (ctypes.c_int, [_p])
+_SIGS["lifted_batch_plan_create_nd_f32"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p])
+_SIGS["lifted_batch_plan_create_nd_f64"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p])
 _SIGS["lifted_lwt_batch_nd_f32"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
 _SIGS["lifted_lwt_batch_nd_f64"] = (ctypes.c_int, [_u32, _u32, _sz, _p, _p, _p, _p])
 _SIGS["lifted_blur2d_f32"] = (ctypes.c_int, [_p, _p, _sz, _sz, _sz, _p, _sz, ctypes.c_int, _p])

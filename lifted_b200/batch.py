@@ -28,8 +28,9 @@ from .pylifted import Transform, resolve_mode, resolve_wavelet
 
 ITEM_FIELDS = ("kind", "prog", "sig", "lev0", "nlev", "src_sel", "dst_sel",
                "wait_ctr", "wait_target", "done_ctr", "n0", "in_off", "out_off",
-               "src_off", "dst_off", "t0", "t1", "halo", "gbuf", "phase")
-KIND_NAMES = ("whole_fwd", "whole_rev", "tile_fwd", "tile_rev")
+               "src_off", "dst_off", "t0", "t1", "halo", "gbuf", "phase", "geo")
+GEO_FIELDS = ("n", "sa", "oshape0", "oshape1", "oshape2", "ostride0", "ostride1", "ostride2")
+KIND_NAMES = ("whole_fwd", "whole_rev", "tile_fwd", "tile_rev", "lines_fwd", "lines_rev")
 
 
 def _torch():
@@ -157,6 +158,18 @@ class BatchPlan:
             out[i] = np.frombuffer(buf, dtype=np.int64)
         return out
 
+    def geometries(self) -> np.ndarray:
+        """Axis-pass geometries of a plan of nD images, one row of GEO_FIELDS
+        each (indexed by the line items' ``geo``)."""
+        out = []
+        lib = _lib.load()
+        buf = (ctypes.c_int64 * len(GEO_FIELDS))()
+        i = 0
+        while lib.lifted_batch_plan_geo(self._plan, i, buf, len(GEO_FIELDS)) == _lib.OK:
+            out.append(np.frombuffer(buf, dtype=np.int64).copy())
+            i += 1
+        return np.array(out, dtype=np.int64).reshape(-1, len(GEO_FIELDS))
+
     def close(self):
         if self._plan:
             _lib.load().lifted_batch_plan_destroy(self._plan)
@@ -214,12 +227,44 @@ def image_table(shapes, wavelets, levels=0, in_offsets=None, out_offsets=None):
     return tab, n
 
 
+class ImagePlan(BatchPlan):
+    """A planned batch of nD images (lifted_batch_plan_create_nd_*): every
+    image, a dense C-order array of 1..4 axes, is transformed separably over
+    all of its axes; one persistent launch per run, whatever the shapes."""
+
+    def __init__(self, shapes, wavelets, levels=0, op=Transform.Forward, mode="Zero",
+                 dtype="float32", in_offsets=None, out_offsets=None,
+                 tuning: dict | None = None):
+        self._plan = ctypes.c_void_p()
+        self.op = int(op)
+        self.mode = resolve_mode(mode)
+        self.dtype_bytes = _dtype_bytes(dtype)
+        tab, n = image_table(shapes, wavelets, levels, in_offsets, out_offsets)
+        self.nsignals = n
+        sizes = np.array([int(np.prod(s)) for s in shapes], dtype=np.int64)
+        ino = np.array([tab[i].in_offset for i in range(n)], dtype=np.int64)
+        outo = np.array([tab[i].out_offset for i in range(n)], dtype=np.int64)
+        self.in_elems = int((ino + sizes).max()) if n else 0
+        self.out_elems = int((outo + sizes).max()) if n else 0
+        tu = None
+        if tuning:
+            tu = _lib.BatchTuning(**{k: int(v) for k, v in tuning.items()})
+        lib = _lib.load()
+        fn = lib.lifted_batch_plan_create_nd_f32 if self.dtype_bytes == 4 else \
+            lib.lifted_batch_plan_create_nd_f64
+        _lib.check(fn(self.op, self.mode, n, ctypes.byref(tab),
+                      ctypes.byref(tu) if tu is not None else None,
+                      ctypes.byref(self._plan)))
+
+
 def lwt_images(images, wavelets, levels=0, op=Transform.Forward, mode="Zero"):
     """Transforms a list of CUDA tensors of differing shapes (each separable
     over all of its axes, as ``pylifted`` would with ``axes=None``) in one C
-    ABI call on the current stream: the images are packed into one buffer,
-    identically shaped neighbours run as one launch per axis.  Returns the
-    list of results (views of one packed output)."""
+    ABI call on the current stream: the images are packed into one buffer
+    and run as one persistent launch, or, for a batch of a few distinct
+    shapes, identically shaped neighbours as one launch per axis (the
+    "batch_nd_mode" option).  Returns the list of results (views of one
+    packed output)."""
     torch = _torch()
     if not images:
         return []

@@ -38,7 +38,21 @@ enum BatchItemKind : int32_t {
   BI_WHOLE_FWD = 0,
   BI_WHOLE_REV = 1,
   BI_TILE_FWD = 2,
-  BI_TILE_REV = 3
+  BI_TILE_REV = 3,
+  BI_LINES_FWD = 4,  // line items of an nD image's axis pass (below)
+  BI_LINES_REV = 5
+};
+
+// Lines of one axis pass of a dense C-order nD image (line items of a
+// batch of nD images): the lines along the axis, enumerated over the other
+// dims fastest first, so consecutive line indices of a strided axis are
+// adjacent in memory.  Element i of line L sits at
+// base(L) + i * sa, base(L) = sum over the other dims of idx_d * ostride_d.
+struct BatchAxisGeom {
+  int64_t n;           // line length
+  int64_t sa;          // element stride along the axis
+  int64_t oshape[3];   // other dims, fastest first (1 where absent)
+  int64_t ostride[3];
 };
 // Where a band lives.
 enum BandSel : int32_t { BS_IN = 0, BS_OUT = 1, BS_SCRATCH = 2 };
@@ -54,15 +68,19 @@ struct BatchItem {
   int32_t wait_ctr;     // completion counter to wait for (-1: none)
   int32_t wait_target;  // value that counter must reach
   int32_t done_ctr;     // counter this item increments when done (-1: none)
-  int64_t n0;           // signal length
+  int32_t geo;          // line items: index of the axis pass's geometry
+  int32_t pad_;
+  int64_t n0;           // signal length (line items: line length)
   int64_t in_off;       // signal offset in `in` (elements)
   int64_t out_off;      // signal offset in `out`
   int64_t src_off;      // offset of the source band in its array
   int64_t dst_off;      // offset of the destination band in its array
-  int64_t t0, t1;       // tile interior, samples of band lev0
+  int64_t t0, t1;       // tile interior, samples of band lev0 (line
+                        // items: the lines [t0, t1) of the pass)
   int64_t halo;         // tile halo per side, samples of band lev0
   int64_t gbuf;         // whole item over global buffers: scratch offset of
-                        // its 1.5 * band elements (-1: shared memory)
+                        // its 1.5 * band elements (-1: shared memory; line
+                        // items: -2 = the CTA's own slot of global scratch)
 };
 
 template <typename T>
@@ -80,6 +98,9 @@ struct BatchParams {
   int64_t buf_elems;   // shared-memory band capacity (elements, 1.5x band)
   int32_t spin_limit;  // polls of a completion counter before giving up
   int32_t pad_;
+  const BatchAxisGeom* geos;  // line items: axis pass geometries
+  int64_t slot_off;    // line items longer than shared memory: CTA b works
+  int64_t slot_elems;  //   in scratch[slot_off + b * slot_elems, ...)
 };
 
 // Shared memory of the batch kernel for a band capacity of `buf_elems`.

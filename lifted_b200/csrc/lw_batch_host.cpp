@@ -44,6 +44,14 @@ struct lifted_batch_plan {
   // device buffers from the stream-ordered pool (plans the library caches
   // for long lines), freed stream-ordered after the last run
   bool pooled = false;
+  // batches of nD images (line items): axis pass geometries, and the
+  // per-CTA global slots of lines longer than shared memory holds
+  bool nd = false;
+  bool nd_inplace_ok = false;  // the table may run with in == out
+  std::vector<lw::BatchAxisGeom> geos;
+  void* d_geos = nullptr;
+  int64_t slot_elems = 0;
+  int64_t slot_off = 0;
   // captured graph of one run and the pointers it was captured with
   cudaGraphExec_t gexec = nullptr;
   const void* g_in = nullptr;
@@ -503,7 +511,19 @@ int ensure_device(lifted_batch_plan* p, cudaStream_t stream = nullptr) {
     if (p->pooled) scratch_free(ptr, stream);
     else cudaFree(ptr);
   };
+  if (p->slot_elems > 0) {
+    // one global slot per resident CTA for line items too long for shared
+    // memory, after the plan's own scratch bands
+    p->slot_off = ((int64_t)(p->scratch_bytes / sizeof(T)) + kBandAlign - 1) / kBandAlign *
+                  kBandAlign;
+    p->slot_elems = (p->slot_elems + kBandAlign - 1) / kBandAlign * kBandAlign;
+    p->scratch_bytes = (size_t)(p->slot_off + (int64_t)p->grid * p->slot_elems) * sizeof(T);
+  }
   e = alloc(&p->d_items, p->items.size() * sizeof(BatchItem));
+  if (e == cudaSuccess && !p->geos.empty())
+    e = alloc(&p->d_geos, p->geos.size() * sizeof(BatchAxisGeom));
+  if (e == cudaSuccess && !p->geos.empty())
+    e = upload(p->d_geos, p->geos.data(), p->geos.size() * sizeof(BatchAxisGeom));
   if (e == cudaSuccess) e = alloc(&p->d_progs, p->progs_bytes);
   if (e == cudaSuccess) e = alloc((void**)&p->d_sync, (size_t)(2 + p->ncounters) * sizeof(int32_t));
   if (e == cudaSuccess && p->scratch_bytes) e = alloc(&p->d_scratch, p->scratch_bytes);
@@ -515,7 +535,8 @@ int ensure_device(lifted_batch_plan* p, cudaStream_t stream = nullptr) {
     release(p->d_progs);
     release(p->d_sync);
     release(p->d_scratch);
-    p->d_items = p->d_progs = p->d_scratch = nullptr;
+    release(p->d_geos);
+    p->d_items = p->d_progs = p->d_scratch = p->d_geos = nullptr;
     p->d_sync = nullptr;
     return set_error(e == cudaErrorMemoryAllocation ? LIFTED_ENOMEM : LIFTED_ECUDA,
                      "batch plan buffers: %s", cudaGetErrorString(e));
@@ -530,16 +551,19 @@ int ensure_device(lifted_batch_plan* p, cudaStream_t stream = nullptr) {
 
 template <typename T>
 int plan_run(lifted_batch_plan* p, const T* in, T* out, cudaStream_t stream,
-             bool count = true) {
+             bool count = true, bool spans_checked = false) {
   if (p->items.empty()) return LIFTED_OK;
   if (!device_pointer(in) || !device_pointer(out))
     return set_error(LIFTED_EINVAL, "batch transforms take device (or managed) pointers");
-  // in and out must not overlap: tiles read input other tiles' outputs would clobber
+  // in and out must not overlap: tiles read input other tiles' outputs would
+  // clobber; a batch of nD images may also run with in == out when every
+  // image is transformed in place
   const char* ib = (const char*)in;
   const char* ie = (const char*)(in + p->max_in);
   const char* ob = (const char*)out;
   const char* oe = (const char*)(out + p->max_out);
-  if (ib < oe && ob < ie)
+  const bool inplace = p->nd && (const void*)in == (const void*)out && p->nd_inplace_ok;
+  if (!spans_checked && !inplace && ib < oe && ob < ie)
     return set_error(LIFTED_EINVAL, "batch input and output overlap");
   int rc = ensure_device<T>(p, stream);
   if (rc) return rc;
@@ -564,6 +588,9 @@ int plan_run(lifted_batch_plan* p, const T* in, T* out, cudaStream_t stream,
   bp.bc = p->bc;
   bp.buf_elems = p->buf_elems;
   bp.spin_limit = p->spin_limit;
+  bp.geos = (const BatchAxisGeom*)p->d_geos;
+  bp.slot_off = p->slot_off;
+  bp.slot_elems = p->slot_elems;
   e = launch_batch(bp, p->grid, p->block, p->smem, stream);
   if (count) {
     count_launches(1);
@@ -711,6 +738,285 @@ template int run_lines_batched<float>(uint32_t, int, int, const LineGeom&, int, 
 template int run_lines_batched<double>(uint32_t, int, int, const LineGeom&, int,
                                        const double*, double*, cudaStream_t);
 
+// ---------------------------------------------------------------------------
+// Batches of nD images (lifted_lwt_batch_nd_*) as one persistent launch.
+//
+// Every image is a dense C-order array transformed separably over all of its
+// axes in order (src/lifted-drivers-inl.hpp:417-486: the first axis reads
+// `in`, later axes work in place on `out`).  Its pass along an axis is cut
+// into line items of W whole lines each; the items of the image's next axis
+// wait (bounded) on a completion counter that the items of this axis
+// increment, and the queue holds every image's first-axis items before any
+// second-axis item, and so on, so every wait ends.  Images of any shape,
+// wavelet and level counts share the launch.
+
+namespace {
+
+template <typename T>
+int plan_create_nd(uint32_t op, uint32_t bc, size_t nimg, const lifted_image_t* ims,
+                   const lifted_batch_tuning_t* tu, lifted_batch_plan** out) {
+  *out = nullptr;
+  if (op > 3) return set_error(LIFTED_EINVAL, "unknown transform %u", op);
+  if (bc > 4) return set_error(LIFTED_EINVAL, "unknown boundary condition %u", bc);
+  // shared-memory budget per CTA (elements) and CTA size: lines of an axis
+  // pass are grouped up to this budget (a line needs 1.5 of its length)
+  const int64_t budget = (tu && tu->whole_max) ? (int64_t)tu->whole_max * 3 / 2
+                                              : (int64_t)(48 * 1024) / (int64_t)sizeof(T);
+  const int block = (tu && tu->block) ? (int)tu->block : 256;
+  if (block < 64 || block > 512 || block % 32)
+    return set_error(LIFTED_EINVAL, "block size %d not in 64..512 (multiple of 32)", block);
+  if (nimg && !ims) return set_error(LIFTED_EINVAL, "null image table");
+  // shapes; outputs pairwise disjoint; whether the table runs in place
+  // (in == out): every image's input span equals its output span or misses
+  // it, and meets no other image's output span
+  struct Span {
+    uint64_t lo, hi;
+    size_t img;
+  };
+  std::vector<Span> outs, ins;
+  for (size_t i = 0; i < nimg; ++i) {
+    const lifted_image_t& im = ims[i];
+    if (im.ndim < 1 || im.ndim > 4)
+      return set_error(LIFTED_EINVAL, "image %zu: ndim %u outside 1..4", i, im.ndim);
+    uint64_t n = 1;
+    for (uint32_t d = 0; d < im.ndim; ++d) {
+      if (im.shape[d] == 0) return set_error(LIFTED_EINVAL, "image %zu: empty axis %u", i, d);
+      if (n > (UINT64_MAX >> 2) / im.shape[d])
+        return set_error(LIFTED_EINVAL, "image %zu: size overflow", i);
+      n *= im.shape[d];
+    }
+    outs.push_back({im.out_offset, im.out_offset + n, i});
+    ins.push_back({im.in_offset, im.in_offset + n, i});
+  }
+  std::sort(outs.begin(), outs.end(), [](const Span& a, const Span& b) { return a.lo < b.lo; });
+  for (size_t k = 1; k < outs.size(); ++k)
+    if (outs[k].lo < outs[k - 1].hi)
+      return set_error(LIFTED_EINVAL, "images %zu and %zu have overlapping outputs",
+                       outs[k - 1].img, outs[k].img);
+  bool inplace_ok = true;
+  for (const Span& a : ins) {
+    auto it = std::upper_bound(outs.begin(), outs.end(), a.lo,
+                               [](uint64_t v, const Span& o) { return v < o.hi; });
+    for (; it != outs.end() && it->lo < a.hi && inplace_ok; ++it)
+      if (it->img != a.img || it->lo != a.lo) inplace_ok = false;
+  }
+  auto plan = std::make_unique<lifted_batch_plan>();
+  plan->dtype = (int)sizeof(T);
+  plan->op = (int)op;
+  plan->bc = (int)bc;
+  plan->nd = true;
+  plan->nd_inplace_ok = inplace_ok;
+  plan->nsignals = (int64_t)nimg;
+  std::map<uint32_t, int> pidx;
+  std::vector<DevProgram<T>> dprogs;
+  std::vector<BatchItem>& items = plan->items;
+  std::vector<int32_t>& phase = plan->item_phase;
+  std::vector<int64_t> work;
+  int64_t buf = 0;
+  int32_t nctr = 0;
+  const bool fwd = (op == TF_F || op == TF_IA);
+  for (size_t ii = 0; ii < nimg; ++ii) {
+    const lifted_image_t& im = ims[ii];
+    Program pr;
+    int rc = catalogue_program(im.wavelet, &pr);
+    if (rc) return set_error(rc, "image %zu: unknown wavelet value %u", ii, im.wavelet);
+    int pi;
+    auto f = pidx.find(im.wavelet);
+    if (f == pidx.end()) {
+      DevProgram<T> dp;
+      resolve_program<T>(pr, (int)op, /*across=*/1, &dp);
+      pi = (int)dprogs.size();
+      pidx[im.wavelet] = pi;
+      dprogs.push_back(dp);
+    } else {
+      pi = f->second;
+    }
+    const size_t nd = im.ndim;
+    size_t shape[4], axes[4], lv_in[4];
+    int64_t stride[4];
+    int64_t numel = 1;
+    for (size_t d = 0; d < nd; ++d) {
+      shape[d] = (size_t)im.shape[d];
+      axes[d] = d;
+      lv_in[d] = im.levels[d];
+      numel *= (int64_t)im.shape[d];
+    }
+    int64_t st = 1;
+    for (size_t d = nd; d-- > 0;) {
+      stride[d] = st;
+      st *= (int64_t)shape[d];
+    }
+    std::vector<size_t> lv;
+    rc = resolve_sep_levels(pr, op, bc, shape, nd, axes, lv_in, &lv);
+    if (rc) return set_error(rc, "image %zu: %s", ii, last_error());
+    plan->max_in = std::max<int64_t>(plan->max_in, (int64_t)im.in_offset + numel);
+    plan->max_out = std::max<int64_t>(plan->max_out, (int64_t)im.out_offset + numel);
+    // axes that run (levels > 0), in order
+    std::vector<size_t> run;
+    for (size_t a = 0; a < nd; ++a)
+      if (lv[a] > 0) run.push_back(a);
+    int32_t prev = -1, prev_n = 0;
+    for (size_t k = 0; k < run.size(); ++k) {
+      const size_t a = run[k];
+      const int64_t n = (int64_t)shape[a];
+      BatchAxisGeom g;
+      std::memset(&g, 0, sizeof(g));
+      g.n = n;
+      g.sa = stride[a];
+      int no = 0;
+      for (size_t d = nd; d-- > 0;) {
+        if (d == a) continue;
+        g.oshape[no] = (int64_t)shape[d];
+        g.ostride[no] = stride[d];
+        ++no;
+      }
+      for (; no < 3; ++no) {
+        g.oshape[no] = 1;
+        g.ostride[no] = 0;
+      }
+      const int32_t gi = (int32_t)plan->geos.size();
+      plan->geos.push_back(g);
+      const int64_t nlines = numel / n;
+      const int64_t need = n + (n - n / 2);
+      const bool strided = g.sa != 1;
+      int64_t W;
+      int64_t gbuf = -1;
+      if (need > budget) {
+        W = 1;
+        gbuf = -2;
+        plan->slot_elems = std::max(plan->slot_elems, need);
+        plan->nwhole_global++;
+      } else {
+        const int64_t want = strided ? 32 : std::max<int64_t>(1, 4096 / n);
+        W = std::min<int64_t>({want, budget / need, nlines});
+        W = std::max<int64_t>(W, 1);
+        buf = std::max(buf, W * need);
+      }
+      const int64_t nit = (nlines + W - 1) / W;
+      if (nit > (int64_t)INT32_MAX / 2 || (int64_t)items.size() + nit > (int64_t)INT32_MAX / 2)
+        return set_error(LIFTED_EINVAL, "image %zu: too many line items", ii);
+      const int32_t ctr = k + 1 < run.size() ? nctr++ : -1;
+      for (int64_t t = 0; t < nit; ++t) {
+        BatchItem it;
+        std::memset(&it, 0, sizeof(it));
+        it.kind = fwd ? BI_LINES_FWD : BI_LINES_REV;
+        it.prog = pi;
+        it.sig = (int32_t)ii;
+        it.lev0 = 0;
+        it.nlev = (int32_t)lv[a];
+        it.src_sel = a == 0 ? BS_IN : BS_OUT;
+        it.dst_sel = BS_OUT;
+        it.wait_ctr = prev;
+        it.wait_target = prev_n;
+        it.done_ctr = ctr;
+        it.geo = gi;
+        it.n0 = n;
+        it.in_off = (int64_t)im.in_offset;
+        it.out_off = (int64_t)im.out_offset;
+        it.src_off = it.src_sel == BS_IN ? it.in_off : it.out_off;
+        it.dst_off = it.out_off;
+        it.t0 = t * W;
+        it.t1 = std::min(nlines, (t + 1) * W);
+        it.gbuf = gbuf;
+        items.push_back(it);
+        phase.push_back((int32_t)k);
+        work.push_back((it.t1 - it.t0) * n);
+        plan->nwhole++;
+      }
+      prev = ctr;
+      prev_n = (int32_t)nit;
+    }
+  }
+  // queue order: by axis position (every producer before its consumers),
+  // then largest work first
+  std::vector<size_t> ord(items.size());
+  for (size_t i = 0; i < ord.size(); ++i) ord[i] = i;
+  std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+    if (phase[a] != phase[b]) return phase[a] < phase[b];
+    return work[a] > work[b];
+  });
+  {
+    std::vector<BatchItem> it2(items.size());
+    std::vector<int32_t> ph2(items.size());
+    for (size_t i = 0; i < ord.size(); ++i) {
+      it2[i] = items[ord[i]];
+      ph2[i] = phase[ord[i]];
+    }
+    items.swap(it2);
+    phase.swap(ph2);
+  }
+  plan->ncounters = nctr;
+  plan->buf_elems = std::max<int64_t>(buf, 3 * 64);
+  plan->buf_elems = (plan->buf_elems + 3) / 3 * 3;
+  plan->smem = batch_smem_bytes<T>(plan->buf_elems);
+  if (plan->smem > kMaxDynSmem)
+    return set_error(LIFTED_EINVAL, "line items need %zu bytes of shared memory (limit %zu)",
+                     plan->smem, kMaxDynSmem);
+  plan->block = block;
+  if (tu && tu->spin_limit) plan->spin_limit = tu->spin_limit > 0 ? tu->spin_limit : 0;
+  plan->scratch_bytes = 0;
+  plan->progs_bytes = dprogs.size() * sizeof(DevProgram<T>);
+  plan->progs_host.assign((const char*)dprogs.data(),
+                          (const char*)dprogs.data() + plan->progs_bytes);
+  *out = plan.release();
+  return LIFTED_OK;
+}
+
+std::mutex g_nd_mu;
+std::map<std::string, lifted_batch_plan*> g_nd_plans;
+std::vector<std::string> g_nd_order;  // insertion order, oldest first
+constexpr size_t kNdPlans = 8;
+
+}  // namespace
+
+template <typename T>
+int run_batch_nd(uint32_t op, uint32_t bc, size_t nimg, const lifted_image_t* ims, const T* in,
+                 T* out, cudaStream_t stream, bool* ran) {
+  *ran = false;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(LIFTED_ECUDA, "no CUDA device");
+  }
+  std::string key;
+  key.reserve(64 + nimg * sizeof(lifted_image_t));
+  char hdr[64];
+  std::snprintf(hdr, sizeof(hdr), "%d|%d|%u|%u|", dev, (int)sizeof(T), op, bc);
+  key = hdr;
+  key.append((const char*)ims, nimg * sizeof(lifted_image_t));
+  std::lock_guard<std::mutex> lk(g_nd_mu);
+  lifted_batch_plan* plan = nullptr;
+  auto it = g_nd_plans.find(key);
+  if (it != g_nd_plans.end()) {
+    plan = it->second;
+  } else {
+    // a new plan allocates: not inside a stream capture
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) cudaGetLastError();
+    if (cap != cudaStreamCaptureStatusNone) return LIFTED_OK;
+    const int rc = plan_create_nd<T>(op, bc, nimg, ims, nullptr, &plan);
+    if (rc) return rc;
+    plan->pooled = true;
+    if (g_nd_plans.size() >= kNdPlans) {
+      const std::string old = g_nd_order.front();
+      g_nd_order.erase(g_nd_order.begin());
+      lifted_batch_plan* victim = g_nd_plans[old];
+      g_nd_plans.erase(old);
+      lifted_batch_plan_destroy(victim);  // stream-ordered after its last run
+    }
+    g_nd_plans[key] = plan;
+    g_nd_order.push_back(key);
+  }
+  *ran = true;
+  // the caller checked every image's input against the other images' outputs
+  return plan_run<T>(plan, in, out, stream, /*count=*/true, /*spans_checked=*/true);
+}
+
+template int run_batch_nd<float>(uint32_t, uint32_t, size_t, const lifted_image_t*,
+                                 const float*, float*, cudaStream_t, bool*);
+template int run_batch_nd<double>(uint32_t, uint32_t, size_t, const lifted_image_t*,
+                                  const double*, double*, cudaStream_t, bool*);
+
 namespace {
 
 // ---------------------------------------------------------------------------
@@ -822,6 +1128,23 @@ LIFTED_CAPI int lifted_batch_plan_create_f64(uint32_t op, uint32_t bc, size_t ns
   return lw::plan_create<double>(op, bc, nsignals, signals, tuning, plan);
 }
 
+LIFTED_CAPI int lifted_batch_plan_create_nd_f32(uint32_t op, uint32_t bc, size_t nimages,
+                                                const lifted_image_t* images,
+                                                const lifted_batch_tuning_t* tuning,
+                                                lifted_batch_plan_t** plan) {
+  lw::clear_error();
+  if (!plan) return lw::set_error(LIFTED_EINVAL, "null plan pointer");
+  return lw::plan_create_nd<float>(op, bc, nimages, images, tuning, plan);
+}
+LIFTED_CAPI int lifted_batch_plan_create_nd_f64(uint32_t op, uint32_t bc, size_t nimages,
+                                                const lifted_image_t* images,
+                                                const lifted_batch_tuning_t* tuning,
+                                                lifted_batch_plan_t** plan) {
+  lw::clear_error();
+  if (!plan) return lw::set_error(LIFTED_EINVAL, "null plan pointer");
+  return lw::plan_create_nd<double>(op, bc, nimages, images, tuning, plan);
+}
+
 LIFTED_CAPI int lifted_batch_run(lifted_batch_plan_t* plan, const void* in, void* out,
                                  void* stream) {
   lw::clear_error();
@@ -875,7 +1198,19 @@ LIFTED_CAPI int lifted_batch_plan_item(const lifted_batch_plan_t* plan, size_t i
   const int64_t v[] = {it.kind, it.prog, it.sig, it.lev0, it.nlev, it.src_sel,
                        it.dst_sel, it.wait_ctr, it.wait_target, it.done_ctr,
                        it.n0, it.in_off, it.out_off, it.src_off, it.dst_off,
-                       it.t0, it.t1, it.halo, it.gbuf, plan->item_phase[index]};
+                       it.t0, it.t1, it.halo, it.gbuf, plan->item_phase[index], it.geo};
+  const size_t n = sizeof(v) / sizeof(v[0]);
+  for (size_t i = 0; i < nfields && i < n; ++i) fields[i] = v[i];
+  return LIFTED_OK;
+}
+
+LIFTED_CAPI int lifted_batch_plan_geo(const lifted_batch_plan_t* plan, size_t index,
+                                      int64_t* fields, size_t nfields) {
+  if (!plan || !fields) return set_error(LIFTED_EINVAL, "null argument");
+  if (index >= plan->geos.size()) return set_error(LIFTED_EINVAL, "geometry index out of range");
+  const lw::BatchAxisGeom& g = plan->geos[index];
+  const int64_t v[] = {g.n, g.sa, g.oshape[0], g.oshape[1], g.oshape[2],
+                       g.ostride[0], g.ostride[1], g.ostride[2]};
   const size_t n = sizeof(v) / sizeof(v[0]);
   for (size_t i = 0; i < nfields && i < n; ++i) fields[i] = v[i];
   return LIFTED_OK;
@@ -884,7 +1219,7 @@ LIFTED_CAPI int lifted_batch_plan_item(const lifted_batch_plan_t* plan, size_t i
 LIFTED_CAPI void lifted_batch_plan_destroy(lifted_batch_plan_t* plan) {
   if (!plan) return;
   if (plan->gexec) cudaGraphExecDestroy(plan->gexec);
-  void* bufs[4] = {plan->d_items, plan->d_progs, plan->d_sync, plan->d_scratch};
+  void* bufs[5] = {plan->d_items, plan->d_progs, plan->d_sync, plan->d_scratch, plan->d_geos};
   if (plan->pooled) {
     // free on the legacy stream after the plan's last run
     if (plan->last) cudaStreamWaitEvent(nullptr, plan->last, 0);

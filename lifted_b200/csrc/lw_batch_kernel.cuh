@@ -352,6 +352,108 @@ __device__ void whole_rev(const BatchParams<T>& p, const BatchItem& w,
     dst[i] = A[(i & 1) ? ns + (i >> 1) : (i >> 1)];
 }
 
+// Element offset of line L of an nD axis pass (BatchAxisGeom).
+__device__ __forceinline__ int64_t axis_line_base(const BatchAxisGeom& g, int64_t L) {
+  const int64_t i0 = L % g.oshape[0];
+  const int64_t r = L / g.oshape[0];
+  const int64_t i1 = r % g.oshape[1];
+  const int64_t i2 = r / g.oshape[1];
+  return i0 * g.ostride[0] + i1 * g.ostride[1] + i2 * g.ostride[2];
+}
+
+// Line (j) and position (i) of flat index f over W lines of n elements:
+// strided axes walk the lines fastest (adjacent lines are adjacent in
+// memory), contiguous axes walk the positions fastest.
+__device__ __forceinline__ void line_pos(int64_t f, int64_t n, int W, bool strided, int& j,
+                                         int64_t& i) {
+  if (strided) {
+    i = f / W;
+    j = (int)(f - i * W);
+  } else {
+    j = (int)(f / n);
+    i = f - (int64_t)j * n;
+  }
+}
+
+// Line item, forward-stepping: lines [t0, t1) of an nD image's axis pass,
+// every level of the axis, with the exact general step code over W lines at
+// once (the line kernel's multi-line form: src/lifted-drivers-inl.hpp:
+// 75-142 per line).  A holds the lines (pitch n), B their split buffers.
+// The source is `in` for the image's first axis and `out` (in place) for
+// the later ones (src/lifted-drivers-inl.hpp:459-485).
+template <typename T>
+__device__ void lines_fwd(const BatchParams<T>& p, const BatchItem& w,
+                          const DevProgram<T>& prog, T* A, int bc) {
+  const int tid = threadIdx.x;
+  const int nth = blockDim.x;
+  const BatchAxisGeom& g = p.geos[w.geo];
+  const int64_t n = w.n0, nd = n / 2, ns = n - nd;
+  const int W = (int)(w.t1 - w.t0);
+  const bool strided = g.sa != 1;
+  const bool smem = w.gbuf == -1;
+  T* B = A + (int64_t)W * n;
+  const T* src = w.src_sel == BS_IN ? p.in + w.in_off : p.out + w.out_off;
+  const int64_t tot = (int64_t)W * n;
+  for (int64_t f = tid; f < tot; f += nth) {
+    int j;
+    int64_t i;
+    line_pos(f, n, W, strided, j, i);
+    const T* q = src + axis_line_base(g, w.t0 + j) + i * g.sa;
+    T* d = A + (int64_t)j * n + ((i & 1) ? ns + (i >> 1) : (i >> 1));
+    if (smem && w.src_sel == BS_IN) cp_elem(d, q);
+    else *d = w.src_sel == BS_IN ? __ldg(q) : __ldcg(q);
+  }
+  if (smem) cp_wait();
+  __syncthreads();
+  run_program(prog, bc, A, n, W, ns, nd);
+  if (w.nlev > 1) coarse_forward(prog, bc, A, n, B, ns, W, ns, w.nlev - 1);
+  T* dst = p.out + w.out_off;
+  for (int64_t f = tid; f < tot; f += nth) {
+    int j;
+    int64_t i;
+    line_pos(f, n, W, strided, j, i);
+    dst[axis_line_base(g, w.t0 + j) + i * g.sa] = A[(int64_t)j * n + i];
+  }
+}
+
+// Line item, reverse-stepping: from [a_L | d_L | ... | d_1] along each line
+// back to the signal domain (src/lifted-drivers-inl.hpp:182-274 per line).
+template <typename T>
+__device__ void lines_rev(const BatchParams<T>& p, const BatchItem& w,
+                          const DevProgram<T>& prog, T* A, int bc) {
+  const int tid = threadIdx.x;
+  const int nth = blockDim.x;
+  const BatchAxisGeom& g = p.geos[w.geo];
+  const int64_t n = w.n0, nd = n / 2, ns = n - nd;
+  const int W = (int)(w.t1 - w.t0);
+  const bool strided = g.sa != 1;
+  const bool smem = w.gbuf == -1;
+  T* B = A + (int64_t)W * n;
+  const T* src = w.src_sel == BS_IN ? p.in + w.in_off : p.out + w.out_off;
+  const int64_t tot = (int64_t)W * n;
+  for (int64_t f = tid; f < tot; f += nth) {
+    int j;
+    int64_t i;
+    line_pos(f, n, W, strided, j, i);
+    const T* q = src + axis_line_base(g, w.t0 + j) + i * g.sa;
+    T* d = A + (int64_t)j * n + i;
+    if (smem && w.src_sel == BS_IN) cp_elem(d, q);
+    else *d = w.src_sel == BS_IN ? __ldg(q) : __ldcg(q);
+  }
+  if (smem) cp_wait();
+  __syncthreads();
+  if (w.nlev > 1) coarse_reverse(prog, bc, A, n, B, ns, W, ns, w.nlev - 1);
+  run_program(prog, bc, A, n, W, ns, nd);
+  T* dst = p.out + w.out_off;
+  for (int64_t f = tid; f < tot; f += nth) {
+    int j;
+    int64_t i;
+    line_pos(f, n, W, strided, j, i);
+    dst[axis_line_base(g, w.t0 + j) + i * g.sa] =
+        A[(int64_t)j * n + ((i & 1) ? ns + (i >> 1) : (i >> 1))];
+  }
+}
+
 }  // namespace batch
 
 template <typename T>
@@ -406,6 +508,16 @@ __global__ void __launch_bounds__(512)
           break;
         case BI_WHOLE_FWD:
           batch::whole_fwd(p, w, *prog, A, p.bc);
+          break;
+        case BI_LINES_FWD:
+          batch::lines_fwd(p, w, *prog,
+                           w.gbuf == -2 ? p.scratch + p.slot_off + blockIdx.x * p.slot_elems : buf,
+                           p.bc);
+          break;
+        case BI_LINES_REV:
+          batch::lines_rev(p, w, *prog,
+                           w.gbuf == -2 ? p.scratch + p.slot_off + blockIdx.x * p.slot_elems : buf,
+                           p.bc);
           break;
         default:
           batch::whole_rev(p, w, *prog, A, p.bc);

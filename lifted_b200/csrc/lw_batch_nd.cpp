@@ -8,12 +8,22 @@
 //     lifted_lwt_sep_xxx(wavelet, op, bc, ndim, shape, dense strides,
 //                        ndim, {0, .., ndim-1}, levels, in + in_offset,
 //                        out + out_offset, stream)
-// would transform it.  Consecutive table entries with the same wavelet,
-// shape and levels, packed back to back in both buffers, form one group that
-// runs as one separable call over a (group, shape...) view, so a batch of a
-// few distinct shapes costs a few launches per axis whatever its image
-// count; every launch is stream-ordered and can be captured into a CUDA
-// graph.
+// would transform it.  Two ways to run a batch:
+//   persistent  one launch of the batch engine for the whole batch: every
+//               (image, axis) pass is cut into line items on the device
+//               queue, and an image's later axes wait on its earlier ones
+//               through completion counters (lw_batch_host.cpp,
+//               run_batch_nd); images of every shape share the launch;
+//   grouped     consecutive table entries with the same wavelet, shape and
+//               levels, packed back to back in both buffers, form one group
+//               that runs as one separable call over a (group, shape...)
+//               view on the fast per-axis kernels: a few launches per axis
+//               and group.
+// The "batch_nd_mode" option picks one (0: automatic, the persistent launch
+// once the batch has more than kGroupedMax groups; 1: persistent; 2:
+// grouped).  Both are stream-ordered and can be captured into a CUDA graph
+// (the persistent plan is built and cached on the first call outside a
+// capture; a capture that meets an uncached batch runs it grouped).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,6 +36,9 @@
 
 namespace lw {
 namespace {
+
+// Largest number of groups the automatic mode still runs grouped.
+constexpr size_t kGroupedMax = 4;
 
 uint64_t numel_of(const lifted_image_t& im) {
   uint64_t n = 1;
@@ -91,6 +104,32 @@ int batch_nd(uint32_t op, uint32_t bc, size_t nimg, const lifted_image_t* ims, c
                          it->img);
   }
   // groups of consecutive, identically shaped, packed images
+  size_t ngroups = 0;
+  for (size_t i = 0; i < nimg;) {
+    const uint64_t n = numel_of(ims[i]);
+    size_t j = i + 1;
+    while (j < nimg && same_kind(ims[i], ims[j]) &&
+           ims[j].in_offset == ims[j - 1].in_offset + n &&
+           ims[j].out_offset == ims[j - 1].out_offset + n)
+      ++j;
+    ++ngroups;
+    i = j;
+  }
+  const int mode = batch_nd_mode();
+  bool persistent = mode == 1 || (mode == 0 && ngroups > kGroupedMax);
+  // line items run an image in place only when its input and output spans
+  // coincide or are disjoint
+  for (size_t k = 0; k < nimg && persistent; ++k) {
+    const char* lo = ib + ims[k].in_offset * sizeof(T);
+    const char* o = ob + ims[k].out_offset * sizeof(T);
+    const size_t bytes = numel_of(ims[k]) * sizeof(T);
+    if (lo != o && lo < o + bytes && o < lo + bytes) persistent = false;
+  }
+  if (persistent) {
+    bool ran = false;
+    const int rc = run_batch_nd<T>(op, bc, nimg, ims, in, out, (cudaStream_t)stream, &ran);
+    if (rc != LIFTED_OK || ran) return rc;
+  }
   size_t i = 0;
   while (i < nimg) {
     const lifted_image_t& a = ims[i];

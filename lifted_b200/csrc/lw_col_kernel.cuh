@@ -63,6 +63,10 @@ struct ColParams {
   int32_t spin_limit;   // mbarrier polls before giving up
   int32_t stack;        // whole lines of 512/stack samples: a tile stacks
                         // `stack` consecutive outer slices (1: off)
+  int32_t row_order;    // tiles numbered row tile major: CTAs that run at
+                        // the same time read neighbouring strips of the
+                        // same rows (else strip major)
+  int32_t pad_;
   int32_t* err;         // set to 1 when a staging wait gave up
 };
 
@@ -128,8 +132,14 @@ __device__ __forceinline__ TileCoord decode(const ColParams<T>& p, int64_t t) {
   TileCoord c;
   c.outer = t / per_outer;
   const int64_t rem = t - c.outer * per_outer;
-  const int64_t strip = rem / p.ntr;
-  c.rt = rem - strip * p.ntr;
+  int64_t strip;
+  if (p.row_order) {
+    c.rt = rem / nstrips;
+    strip = rem - c.rt * nstrips;
+  } else {
+    strip = rem / p.ntr;
+    c.rt = rem - strip * p.ntr;
+  }
   c.col0 = strip * COL_LANES * V;
   c.wstart = c.rt * p.r.tile - p.r.halo;
   c.outer *= p.stack;  // first slice of the tile's group

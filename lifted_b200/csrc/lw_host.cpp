@@ -84,6 +84,8 @@ std::atomic<int64_t> g_opt_overlap{1};
 std::atomic<int64_t> g_opt_row_windows{1};
 std::atomic<int64_t> g_opt_generic{1};
 std::atomic<int64_t> g_opt_l2_hints{0};
+std::atomic<int64_t> g_opt_col_row_order{1};
+std::atomic<int64_t> g_opt_batch_nd_mode{0};
 
 }  // namespace
 
@@ -859,6 +861,11 @@ int set_option(const char* name, int64_t value) {
     g_opt_generic = value ? 1 : 0;
   } else if (!std::strcmp(name, "l2_hints")) {
     g_opt_l2_hints = value ? 1 : 0;
+  } else if (!std::strcmp(name, "col_row_order")) {
+    g_opt_col_row_order = value ? 1 : 0;
+  } else if (!std::strcmp(name, "batch_nd_mode")) {
+    if (value < 0 || value > 2) return set_error(LIFTED_EINVAL, "batch_nd_mode outside 0..2");
+    g_opt_batch_nd_mode = value;
   } else if (!std::strcmp(name, "max_global_ctas")) {
     if (value < 1 || value > 65535)
       return set_error(LIFTED_EINVAL, "max_global_ctas outside 1..65535");
@@ -872,6 +879,8 @@ uint64_t launch_count() { return g_launches.load(); }
 bool col_enabled() { return g_opt_tma_strided.load() != 0; }
 bool col_packed() { return g_opt_tma_packed.load() != 0; }
 bool col_stacked() { return g_opt_tma_stacked.load() != 0; }
+bool col_row_order() { return g_opt_col_row_order.load() != 0; }
+int batch_nd_mode() { return (int)g_opt_batch_nd_mode.load(); }
 bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
 bool pdl_enabled() { return g_opt_overlap.load() != 0; }
 bool wtile_enabled() { return g_opt_row_windows.load() != 0; }

@@ -76,6 +76,22 @@ size_t wavelet_width(uint32_t w);
 // Runs the lines of an axis pass (contiguous, non-negative offsets) as a
 // cached batch plan of the batch engine, one signal per line: 1 done, 0 not
 // eligible, -1 failed (the error is set).
+// Runs a batch of nD images (dense C-order, each transformed separably over
+// all of its axes) as one persistent launch of line items, from a cached
+// plan.  Returns a status; *ran is false (and the status LIFTED_OK) when it
+// did not run because a new plan would have to be built inside a stream
+// capture.
+template <typename T>
+int run_batch_nd(uint32_t op, uint32_t bc, size_t nimg, const lifted_image_t* ims, const T* in,
+                 T* out, cudaStream_t stream, bool* ran);
+// The "batch_nd_mode" option: 0 automatic, 1 persistent, 2 grouped.
+int batch_nd_mode();
+// Per-axis levels of the separable driver, resolved and checked (level 0 =
+// max_level; degenerate bands refused), as lifted_lwt_sep_* does.
+int resolve_sep_levels(const Program& prog, uint32_t op, uint32_t bc,
+                       const size_t* shape, size_t naxes, const size_t* axes,
+                       const size_t* levels, std::vector<size_t>* lv);
+
 template <typename T>
 int run_lines_batched(uint32_t wavelet, int op, int bc, const LineGeom& g, int levels,
                       const T* in, T* out, cudaStream_t stream);

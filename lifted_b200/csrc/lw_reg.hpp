@@ -45,6 +45,9 @@ bool col_packed();
 // Whether short strided lines of a 3D view stack several outer slices in
 // one staging window (the "tma_stacked" option).
 bool col_stacked();
+// Whether its tiles run in row-tile-major order (the "col_row_order"
+// option).
+bool col_row_order();
 // Synchronises `stream`; returns 1 (and clears it) if a TMA-staged kernel
 // gave up waiting for a staging copy since the last check, 0 if not, -1 if
 // the check itself failed.

@@ -733,6 +733,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     cp.rank3 = rank == 3;
     cp.a_from_tmp = more ? 1 : 0;
     cp.spin_limit = 1 << 22;
+    cp.row_order = col_row_order() ? 1 : 0;
     cp.err = err;
     const int hmax = wide ? kGenWideHmax
                      : gen ? kGenHmax

@@ -29,9 +29,12 @@ def _fixed(s, d, op, bc, wavelet):
     assert rc == 0, rc
 
 
-def emulate(items, op, bc, prog_wavelets, x, out_elems, scratch_elems, done=None):
+def emulate(items, op, bc, prog_wavelets, x, out_elems, scratch_elems, done=None, geos=None):
     """Runs the items; returns (out, scratch).  ``done`` collects completed
-    counter increments to check every wait is satisfied when reached."""
+    counter increments to check every wait is satisfied when reached.
+    ``geos``: the axis-pass geometries of a plan of nD images (line items:
+    each line of the item is the oracle's 1D transform of that line, read
+    from ``x`` for an image's first axis and in place from ``out`` after)."""
     dt = x.dtype
     out = np.zeros(max(out_elems, 1), dt)
     scratch = np.zeros(max(scratch_elems, 1), dt)
@@ -46,7 +49,20 @@ def emulate(items, op, bc, prog_wavelets, x, out_elems, scratch_elems, done=None
                 ("item runs before its producers", f)
         lev0, nlev = f["lev0"], f["nlev"]
         m = band_len(f["n0"], lev0)
-        if kind == "whole_fwd":
+        if kind in ("lines_fwd", "lines_rev"):
+            g = geos[f["geo"]]
+            n, sa, osh, ost = int(g[0]), int(g[1]), g[2:5], g[5:8]
+            src = x[f["in_off"]:] if f["src_sel"] == 0 else out[f["out_off"]:]
+            dst = out[f["out_off"]:]
+            idx = np.arange(n) * sa
+            for L in range(f["t0"], f["t1"]):
+                i0, r = L % osh[0], L // osh[0]
+                base = int(i0 * ost[0] + (r % osh[1]) * ost[1] + (r // osh[1]) * ost[2])
+                line = src[base + idx].copy()
+                rc, y = po.oracle_sep(line, w, op, bc, [0], [nlev])
+                assert rc == 0, rc
+                dst[base + idx] = y
+        elif kind == "whole_fwd":
             src = arrs[f["src_sel"]]
             band = src[f["src_off"]:f["src_off"] + m].copy()
             region = np.empty(m, dt)

@@ -147,3 +147,70 @@ def test_tuning_table_round_trip_and_use(tmp_path):
     bt.tune_clear()
     assert bt.tune_load(str(out)) == 1
     bt.tune_clear()
+
+
+def random_images(seed, count, dtype):
+    """Images of 1..4 axes and differing shapes, wavelets and per-axis
+    levels (0 = max_level), packed back to back."""
+    rng = np.random.default_rng(seed)
+    shapes, ws, lvs = [], [], []
+    for _ in range(count):
+        nd = int(rng.integers(1, 5))
+        shp = tuple(int(v) for v in rng.integers(3, {1: 300, 2: 70, 3: 20, 4: 9}[nd], nd))
+        w = [v for v in WAVELETS if v != 0][int(rng.integers(0, len(WAVELETS) - 1))]
+        # (not Lazy: its level 0 never resolves)
+        width = po.wavelet_width(w)
+        lv = []
+        for n in shp:
+            mx = po.max_level(width, n)
+            lv.append(int(rng.integers(0, max(mx, 1) + 1)))
+        shapes.append(shp)
+        ws.append(w)
+        lvs.append(lv)
+    x = rng.standard_normal(int(sum(np.prod(s) for s in shapes))).astype(dtype)
+    return shapes, ws, lvs, x
+
+
+def oracle_images(x, shapes, ws, lvs, op, bc):
+    out = np.zeros_like(x)
+    off = 0
+    for shp, w, lv in zip(shapes, ws, lvs):
+        sz = int(np.prod(shp))
+        img = x[off:off + sz].reshape(shp).copy()
+        rc, o = po.oracle_sep(img, w, op, bc, list(range(len(shp))), lv)
+        assert rc == 0, (shp, w, lv)
+        out[off:off + sz] = o.reshape(-1)
+        off += sz
+    return out
+
+
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+@pytest.mark.parametrize("bc", [0, 3])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_emulated_image_plan_matches_oracle(op, bc, dtype):
+    """A plan of nD images of all-distinct shapes: its line items, run in
+    queue order by the emulator (every wait satisfied by earlier items),
+    give each image's separable transform over all of its axes; small
+    shared-memory budgets force single lines and global slots."""
+    from lifted_b200.batch import ImagePlan
+
+    shapes, ws, lvs, x = random_images(300 + op + 10 * bc, 24, dtype)
+    want = oracle_images(x, shapes, ws, lvs, op, bc)
+    for tuning in (None, {"whole_max": 64}, {"whole_max": 16, "block": 64}):
+        plan = ImagePlan(shapes, ws, lvs, op=op, mode=bc, dtype=dtype, tuning=tuning)
+        items = plan.items()
+        f = {k: i for i, k in enumerate(ITEM_FIELDS)}
+        assert set(items[:, f["kind"]]) <= {4, 5}
+        got, _ = emulate(items, op, bc, prog_wavelets(ws), x, plan.out_elems, 0,
+                         geos=plan.geometries())
+        assert np.array_equal(got[:len(want)], want), tuning
+        if tuning and tuning["whole_max"] == 16:
+            assert (items[:, f["gbuf"]] == -2).any()
+        plan.close()
+
+
+def test_image_plan_refuses_overlapping_outputs():
+    from lifted_b200.batch import ImagePlan
+
+    with pytest.raises(ValueError):
+        ImagePlan([(8, 8), (8, 8)], "db2", 1, out_offsets=[0, 32])
