@@ -887,7 +887,8 @@ int plan_create_nd(uint32_t op, uint32_t bc, size_t nimg, const lifted_image_t* 
         plan->slot_elems = std::max(plan->slot_elems, need);
         plan->nwhole_global++;
       } else {
-        const int64_t want = strided ? 32 : std::max<int64_t>(1, 4096 / n);
+        // at most 64 lines (the kernel's per-item line table)
+        const int64_t want = strided ? 32 : std::min<int64_t>(64, std::max<int64_t>(1, 4096 / n));
         W = std::min<int64_t>({want, budget / need, nlines});
         W = std::max<int64_t>(W, 1);
         buf = std::max(buf, W * need);

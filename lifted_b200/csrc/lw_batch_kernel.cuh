@@ -361,32 +361,28 @@ __device__ __forceinline__ int64_t axis_line_base(const BatchAxisGeom& g, int64_
   return i0 * g.ostride[0] + i1 * g.ostride[1] + i2 * g.ostride[2];
 }
 
-// Line (j) and position (i) of flat index f over W lines of n elements:
-// strided axes walk the lines fastest (adjacent lines are adjacent in
-// memory), contiguous axes walk the positions fastest.
-__device__ __forceinline__ void line_pos(int64_t f, int64_t n, int W, bool strided, int& j,
-                                         int64_t& i) {
-  if (strided) {
-    i = f / W;
-    j = (int)(f - i * W);
-  } else {
-    j = (int)(f / n);
-    i = f - (int64_t)j * n;
-  }
-}
-
 // Line item, forward-stepping: lines [t0, t1) of an nD image's axis pass,
 // every level of the axis, with the exact general step code over W lines at
 // once (the line kernel's multi-line form: src/lifted-drivers-inl.hpp:
 // 75-142 per line).  A holds the lines (pitch n), B their split buffers.
 // The source is `in` for the image's first axis and `out` (in place) for
 // the later ones (src/lifted-drivers-inl.hpp:459-485).
+// Element offsets of the item's lines (at most kMaxItemLines) in `base`.
+constexpr int kMaxItemLines = 64;
+__device__ __forceinline__ void item_bases(const BatchItem& w, const BatchAxisGeom& g,
+                                           int64_t* base) {
+  const int W = (int)(w.t1 - w.t0);
+  for (int j = threadIdx.x; j < W; j += blockDim.x) base[j] = axis_line_base(g, w.t0 + j);
+  __syncthreads();
+}
+
 template <typename T>
 __device__ void lines_fwd(const BatchParams<T>& p, const BatchItem& w,
-                          const DevProgram<T>& prog, T* A, int bc) {
+                          const DevProgram<T>& prog, T* A, int bc, int64_t* base) {
   const int tid = threadIdx.x;
   const int nth = blockDim.x;
   const BatchAxisGeom& g = p.geos[w.geo];
+  item_bases(w, g, base);
   const int64_t n = w.n0, nd = n / 2, ns = n - nd;
   const int W = (int)(w.t1 - w.t0);
   const bool strided = g.sa != 1;
@@ -398,7 +394,7 @@ __device__ void lines_fwd(const BatchParams<T>& p, const BatchItem& w,
     int j;
     int64_t i;
     line_pos(f, n, W, strided, j, i);
-    const T* q = src + axis_line_base(g, w.t0 + j) + i * g.sa;
+    const T* q = src + base[j] + i * g.sa;
     T* d = A + (int64_t)j * n + ((i & 1) ? ns + (i >> 1) : (i >> 1));
     if (smem && w.src_sel == BS_IN) cp_elem(d, q);
     else *d = w.src_sel == BS_IN ? __ldg(q) : __ldcg(q);
@@ -412,7 +408,7 @@ __device__ void lines_fwd(const BatchParams<T>& p, const BatchItem& w,
     int j;
     int64_t i;
     line_pos(f, n, W, strided, j, i);
-    dst[axis_line_base(g, w.t0 + j) + i * g.sa] = A[(int64_t)j * n + i];
+    dst[base[j] + i * g.sa] = A[(int64_t)j * n + i];
   }
 }
 
@@ -420,10 +416,11 @@ __device__ void lines_fwd(const BatchParams<T>& p, const BatchItem& w,
 // back to the signal domain (src/lifted-drivers-inl.hpp:182-274 per line).
 template <typename T>
 __device__ void lines_rev(const BatchParams<T>& p, const BatchItem& w,
-                          const DevProgram<T>& prog, T* A, int bc) {
+                          const DevProgram<T>& prog, T* A, int bc, int64_t* base) {
   const int tid = threadIdx.x;
   const int nth = blockDim.x;
   const BatchAxisGeom& g = p.geos[w.geo];
+  item_bases(w, g, base);
   const int64_t n = w.n0, nd = n / 2, ns = n - nd;
   const int W = (int)(w.t1 - w.t0);
   const bool strided = g.sa != 1;
@@ -435,7 +432,7 @@ __device__ void lines_rev(const BatchParams<T>& p, const BatchItem& w,
     int j;
     int64_t i;
     line_pos(f, n, W, strided, j, i);
-    const T* q = src + axis_line_base(g, w.t0 + j) + i * g.sa;
+    const T* q = src + base[j] + i * g.sa;
     T* d = A + (int64_t)j * n + i;
     if (smem && w.src_sel == BS_IN) cp_elem(d, q);
     else *d = w.src_sel == BS_IN ? __ldg(q) : __ldcg(q);
@@ -449,8 +446,7 @@ __device__ void lines_rev(const BatchParams<T>& p, const BatchItem& w,
     int j;
     int64_t i;
     line_pos(f, n, W, strided, j, i);
-    dst[axis_line_base(g, w.t0 + j) + i * g.sa] =
-        A[(int64_t)j * n + ((i & 1) ? ns + (i >> 1) : (i >> 1))];
+    dst[base[j] + i * g.sa] = A[(int64_t)j * n + ((i & 1) ? ns + (i >> 1) : (i >> 1))];
   }
 }
 
@@ -465,6 +461,7 @@ __global__ void __launch_bounds__(512)
                                 ((sizeof(DevProgram<T>) + 15) / 16) * 16);
   __shared__ int32_t s_item;
   __shared__ int32_t s_ok;
+  __shared__ int64_t s_base[batch::kMaxItemLines];
   const int64_t cap2 = p.buf_elems / 3;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(p.head, 1);
@@ -512,12 +509,12 @@ __global__ void __launch_bounds__(512)
         case BI_LINES_FWD:
           batch::lines_fwd(p, w, *prog,
                            w.gbuf == -2 ? p.scratch + p.slot_off + blockIdx.x * p.slot_elems : buf,
-                           p.bc);
+                           p.bc, s_base);
           break;
         case BI_LINES_REV:
           batch::lines_rev(p, w, *prog,
                            w.gbuf == -2 ? p.scratch + p.slot_off + blockIdx.x * p.slot_elems : buf,
-                           p.bc);
+                           p.bc, s_base);
           break;
         default:
           batch::whole_rev(p, w, *prog, A, p.bc);

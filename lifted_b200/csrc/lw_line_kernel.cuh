@@ -166,14 +166,35 @@ __device__ void fold_back(const DevStep<T>& st, int bc, T* y, int64_t ny,
 }
 
 // Line j and position i of flat index f over W lines of m elements (no
-// division for a single line).
+// division for a single line).  Several lines are only ever held in shared
+// memory (W * m < 2^31), so a 32-bit division serves them.
 __device__ __forceinline__ void split_index(int64_t f, int64_t m, int W, int& j, int64_t& i) {
   if (W == 1) {
     j = 0;
     i = f;
   } else {
-    j = (int)(f / m);
-    i = f - (int64_t)j * m;
+    const uint32_t q = (uint32_t)f / (uint32_t)m;
+    j = (int)q;
+    i = f - (int64_t)q * m;
+  }
+}
+
+// Line j and position i of flat index f over W lines of n elements, walking
+// the positions fastest (contiguous lines) or the lines fastest (strided
+// lines, adjacent in memory); 32-bit division as in split_index.
+__device__ __forceinline__ void line_pos(int64_t f, int64_t n, int W, bool lines_fastest, int& j,
+                                         int64_t& i) {
+  if (W == 1) {
+    j = 0;
+    i = f;
+  } else if (lines_fastest) {
+    const uint32_t q = (uint32_t)f / (uint32_t)W;
+    i = q;
+    j = (int)((uint32_t)f - q * (uint32_t)W);
+  } else {
+    const uint32_t q = (uint32_t)f / (uint32_t)n;
+    j = (int)q;
+    i = f - (int64_t)q * n;
   }
 }
 
@@ -406,13 +427,7 @@ __global__ void __launch_bounds__(512)
       for (int64_t f = tid; f < tot; f += nth) {
         int j;
         int64_t i;
-        if (along_contig) {
-          j = (int)(f / n);
-          i = f - (int64_t)j * n;
-        } else {
-          i = f / We;
-          j = (int)(f - i * We);
-        }
+        line_pos(f, n, We, !along_contig, j, i);
         T v = p.in[s_bin[j] + i * g.sin];
         A[j * p.pitch + ((i & 1) ? ns0 + (i >> 1) : (i >> 1))] = v;
       }
@@ -423,14 +438,16 @@ __global__ void __launch_bounds__(512)
         if (lvl > 0) {
           const int64_t t2 = (int64_t)We * m;
           for (int64_t f = tid; f < t2; f += nth) {
-            int j = (int)(f / m);
-            int64_t i = f - (int64_t)j * m;
+            int j;
+            int64_t i;
+            split_index(f, m, We, j, i);
             B[j * p.pitch_b + i] = A[j * p.pitch + i];
           }
           __syncthreads();
           for (int64_t f = tid; f < t2; f += nth) {
-            int j = (int)(f / m);
-            int64_t i = f - (int64_t)j * m;
+            int j;
+            int64_t i;
+            split_index(f, m, We, j, i);
             T v = B[j * p.pitch_b + i];
             A[j * p.pitch + ((i & 1) ? ns + (i >> 1) : (i >> 1))] = v;
           }
@@ -443,13 +460,7 @@ __global__ void __launch_bounds__(512)
       for (int64_t f = tid; f < tot; f += nth) {
         int j;
         int64_t i;
-        if (along_contig_out) {
-          j = (int)(f / n);
-          i = f - (int64_t)j * n;
-        } else {
-          i = f / We;
-          j = (int)(f - i * We);
-        }
+        line_pos(f, n, We, !along_contig_out, j, i);
         p.out[s_bout[j] + i * g.sout] = A[j * p.pitch + i];
       }
     } else {
@@ -457,13 +468,7 @@ __global__ void __launch_bounds__(512)
       for (int64_t f = tid; f < tot; f += nth) {
         int j;
         int64_t i;
-        if (along_contig) {
-          j = (int)(f / n);
-          i = f - (int64_t)j * n;
-        } else {
-          i = f / We;
-          j = (int)(f - i * We);
-        }
+        line_pos(f, n, We, !along_contig, j, i);
         A[j * p.pitch + i] = p.in[s_bin[j] + i * g.sin];
       }
       __syncthreads();
@@ -477,14 +482,16 @@ __global__ void __launch_bounds__(512)
         if (lvl > 0) {
           const int64_t t2 = (int64_t)We * m;
           for (int64_t f = tid; f < t2; f += nth) {
-            int j = (int)(f / m);
-            int64_t i = f - (int64_t)j * m;
+            int j;
+            int64_t i;
+            split_index(f, m, We, j, i);
             B[j * p.pitch_b + i] = A[j * p.pitch + i];
           }
           __syncthreads();
           for (int64_t f = tid; f < t2; f += nth) {
-            int j = (int)(f / m);
-            int64_t i = f - (int64_t)j * m;  // output index
+            int j;
+            int64_t i;
+            split_index(f, m, We, j, i);  // output index
             int64_t src = (i & 1) ? ns + (i >> 1) : (i >> 1);
             A[j * p.pitch + i] = B[j * p.pitch_b + src];
           }
@@ -496,13 +503,7 @@ __global__ void __launch_bounds__(512)
       for (int64_t f = tid; f < tot; f += nth) {
         int j;
         int64_t i;
-        if (along_contig_out) {
-          j = (int)(f / n);
-          i = f - (int64_t)j * n;
-        } else {
-          i = f / We;
-          j = (int)(f - i * We);
-        }
+        line_pos(f, n, We, !along_contig_out, j, i);
         int64_t src = (i & 1) ? ns0 + (i >> 1) : (i >> 1);
         p.out[s_bout[j] + i * g.sout] = A[j * p.pitch + src];
       }

@@ -80,7 +80,7 @@ def distinct_shapes(rng, count):
         if rng.random() < 0.8:
             shp = (int(rng.integers(40, 400)), int(rng.integers(40, 400)))
         else:
-            shp = tuple(int(v) for v in rng.integers(16, 64, 3))
+            shp = tuple(int(v) for v in rng.integers(40, 64, 3))
         if shp not in seen:
             seen.add(shp)
             out.append(shp)
@@ -100,8 +100,11 @@ def test_distinct_shapes_one_launch(op, dtype, bc, nd_mode):
     ws = [int(v) for v in rng.choice([2, 4, 100907, 5, 203, 10309], 48)]
     lvs = []
     for shp, w in zip(shapes, ws):
+        # every axis at least one level (an axis of 0 levels leaves `out` as
+        # it was, and lwt_images does not clear it)
         mxs = [po.max_level(po.wavelet_width(w), n) for n in shp]
-        lvs.append([int(rng.integers(1, mx + 1)) if mx >= 1 else 0 for mx in mxs])
+        assert min(mxs) >= 1, (shp, w)
+        lvs.append([int(rng.integers(1, mx + 1)) for mx in mxs])
     xs = [rng.standard_normal(s).astype(dtype) for s in shapes]
     ts = [torch.from_numpy(x).cuda() for x in xs]
     n0, b0 = _lib.launch_count(), _lib.kernel_launches("batch")
