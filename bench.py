@@ -532,6 +532,53 @@ def inverse_section(dev, x, steps: int = 10):
             "ms_per_step": round(ms, 4)}
 
 
+def boundaries_section(dev, x, steps: int = 10):
+    """The headline step (Forward + ForwardAdjoint, 4096^2 float32 CDF 9/7,
+    levels (6, 6)) under every boundary condition, graph-replayed, L2 flushed
+    between replays outside the events: Zero, Constant, Symmetric and Reflect
+    run on the fast kernels (exact band edges), Periodic on the general
+    kernel."""
+    import torch
+    from lifted_b200 import _lib
+    from lifted_b200 import pylifted as pl
+
+    w = torch.empty_like(x)
+    y = torch.empty_like(x)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    out = {"workload": "as the headline under each boundary condition", "unit": "GB/s"}
+    for bc, name in enumerate(("Zero", "Constant", "Periodic", "Symmetric", "Reflect")):
+        def step():
+            pl._lwt(x, WAVELET, bc, 0, AXES, LEVELS, 1, out=w)
+            pl._lwt(w, WAVELET, bc, 2, AXES, LEVELS, 1, out=y)
+
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize(dev)
+        l0 = _lib.kernel_launches("line")
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+            step()
+        general = _lib.kernel_launches("line") - l0
+        n = steps if bc != 2 else 3
+        ts = []
+        for k in range(n):
+            flush.fill_(float(k))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            graph.replay()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        out[name] = {"value": round(BYTES_PER_STEP / ms / 1e6, 3), "ms_per_step": round(ms, 4),
+                     "general_kernel_launches_per_step": general}
+        del graph
+    z = out["Zero"]["ms_per_step"]
+    for name in ("Constant", "Periodic", "Symmetric", "Reflect"):
+        out[name]["time_vs_zero"] = round(out[name]["ms_per_step"] / z, 3)
+    return out
+
+
 def cfg1_section(dev, steps: int = 10):
     """Plain 1D float64: 64 signals of 65536 i.i.d. N(0,1) (seed 1001),
     Daubechies2, 5 levels along axis 1, Zero boundary, Forward then
@@ -724,7 +771,7 @@ def main() -> int:
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched, autograd and least-squares sections")
     ap.add_argument("--section", choices=["inverse", "cfg1", "batched", "batched_nd", "autograd",
-                                          "lsq", "generic"],
+                                          "lsq", "generic", "boundaries"],
                     help="run only this section (one GPU) and print its JSON; for profiling "
                          "its kernels, not a driver line")
     args = ap.parse_args()
@@ -744,9 +791,9 @@ def main() -> int:
     dev = torch.device("cuda", local_rank)
     if args.section:
         sys.path.insert(0, str(ROOT))
-        if args.section == "inverse":
+        if args.section in ("inverse", "boundaries"):
             xi = torch.from_numpy(make_image(SEED)).to(dev)
-            res = inverse_section(dev, xi)
+            res = (inverse_section if args.section == "inverse" else boundaries_section)(dev, xi)
         else:
             fn = {"cfg1": cfg1_section, "batched": batched_section,
                   "batched_nd": batched_nd_section, "generic": generic_section,
@@ -912,9 +959,10 @@ def main() -> int:
                              f"{cores} threads)"}
 
     extras = {"inverse": None, "cfg1_1d_f64": None, "batched": None, "batched_nd": None,
-              "autograd": None, "lsq": None, "generic": None}
+              "autograd": None, "lsq": None, "generic": None, "boundaries": None}
     if world == 1 and not args.no_extras:
         extras["inverse"] = inverse_section(dev, x)
+        extras["boundaries"] = boundaries_section(dev, x)
         extras["cfg1_1d_f64"] = cfg1_section(dev)
         extras["batched"] = batched_section(dev)
         extras["batched_nd"] = batched_nd_section(dev)
@@ -954,6 +1002,7 @@ def main() -> int:
             "batched": extras["batched"],
             "batched_nd": extras["batched_nd"],
             "generic_wavelets": extras["generic"],
+            "boundaries": extras["boundaries"],
             "autograd": extras["autograd"],
             "lsq": extras["lsq"],
         }

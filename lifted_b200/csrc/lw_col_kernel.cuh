@@ -310,6 +310,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   c.has_l = c.r > 0;
   c.has_r = c.r < COL_CHUNKS - 1;
   c.n = p.r.g.n;
+  c.bc = p.r.bc;
   c.pol_st = l2_store_policy(p.r.l2hint);
   // stacked tiles: chunk r holds chunk rr of slice zr (its own line, whose
   // band edges mask the taps that would reach the neighbouring slices)

@@ -242,21 +242,6 @@ bool bad_index_call(int bc, int64_t i, int64_t n) {
   return false;
 }
 
-// The reference's index maps on inputs that pass bad_index_call (so the
-// loops terminate); returns n for "skip".
-int64_t host_bc_index(int bc, int64_t i, int64_t n) {
-  switch (bc) {
-    case BC_ZERO: return (i < 0 || i >= n) ? n : i;
-    case BC_CONSTANT: return i < 0 ? 0 : (i >= n ? n - 1 : i);
-    case BC_PERIODIC: return (int64_t)((uint64_t)i % (uint64_t)n);
-    case BC_SYMMETRIC:
-      while (i >= n || i < 0) i = i < 0 ? -(i + 1) : 2 * (n - 1) - (i - 1);
-      return i;
-    default:
-      while (i >= n || i < 0) i = i < 0 ? -i : 2 * (n - 1) - i;
-      return i;
-  }
-}
 
 // Replays the index computations of one level of one step program (the loop
 // bounds of src/lifted-steps-inl.hpp:500-615, 754-885, 1011-1126) without
@@ -364,6 +349,22 @@ bool dense(size_t ndim, const size_t* shape, const ptrdiff_t* stride) {
 }  // namespace
 
 bool device_pointer(const void* p) { return is_device_pointer(p); }
+
+// The reference's index maps on inputs that pass bad_index_call (so the
+// loops terminate); returns n for "skip".
+int64_t host_bc_index(int bc, int64_t i, int64_t n) {
+  switch (bc) {
+    case BC_ZERO: return (i < 0 || i >= n) ? n : i;
+    case BC_CONSTANT: return i < 0 ? 0 : (i >= n ? n - 1 : i);
+    case BC_PERIODIC: return (int64_t)((uint64_t)i % (uint64_t)n);
+    case BC_SYMMETRIC:
+      while (i >= n || i < 0) i = i < 0 ? -(i + 1) : 2 * (n - 1) - (i - 1);
+      return i;
+    default:
+      while (i >= n || i < 0) i = i < 0 ? -i : 2 * (n - 1) - i;
+      return i;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Axis passes.

@@ -51,6 +51,9 @@ int family_index(const char* name);
 // L2 priority code (lw_cache.cuh) of the fast kernels' loads and stores:
 // evict_first loads and evict_last stores when the "l2_hints" option is on.
 int l2_hint_code();
+// The reference's boundary index maps (src/lifted-common.hpp:719-779) on the
+// host, for inputs on which its loops terminate; n means "skip the tap".
+int64_t host_bc_index(int bc, int64_t i, int64_t n);
 const char* last_error();
 uint64_t launch_count();
 

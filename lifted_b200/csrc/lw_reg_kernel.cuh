@@ -35,6 +35,8 @@
 #include <cstdint>
 
 #include "lw_cache.cuh"
+#include "lw_edge.cuh"
+#include "lw_lanevec.cuh"
 #include "lw_line_kernel.cuh"
 #include "lw_types.hpp"
 
@@ -191,74 +193,11 @@ struct RegParams {
   int32_t coarse_pitch;   // shared coarse buffer: elements per line (A)
   int32_t coarse_pitch_b; // and of its split buffer (B)
   int32_t l2hint;         // L2 priorities of loads and stores (lw_cache.cuh)
+  int32_t bc;             // boundary condition: Zero, or Constant / Symmetric /
+                          // Reflect with exact band edges (lw_edge.cuh)
+  int32_t pad2_;
   DevProgram<T> prog;
 };
-
-// Lane value types: V adjacent lines per lane.  The arithmetic helpers are
-// exact element-wise equivalents of the scalar forms (IEEE round to nearest;
-// packed FP32x2 on sm_100 for float2).
-template <typename T, int V>
-struct LaneVec;
-template <typename T>
-struct LaneVec<T, 1> {
-  using type = T;
-};
-template <>
-struct LaneVec<float, 2> {
-  using type = float2;
-};
-template <>
-struct LaneVec<double, 2> {
-  using type = double2;
-};
-
-__device__ __forceinline__ float vfop(int sub, float c, float x, float y) {
-  return fop(sub, c, x, y);
-}
-__device__ __forceinline__ double vfop(int sub, double c, double x, double y) {
-  return fop(sub, c, x, y);
-}
-__device__ __forceinline__ float2 vfop(int sub, float c, float2 x, float2 y) {
-  const float cc = sub ? -c : c;
-  return __ffma2_rn(make_float2(cc, cc), x, y);
-}
-__device__ __forceinline__ double2 vfop(int sub, double c, double2 x, double2 y) {
-  return make_double2(fop(sub, c, x.x, y.x), fop(sub, c, x.y, y.y));
-}
-__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
-__device__ __forceinline__ double vadd(double a, double b) { return a + b; }
-__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ double2 vadd(double2 a, double2 b) {
-  return make_double2(a.x + b.x, a.y + b.y);
-}
-__device__ __forceinline__ float vsub(float a, float b) { return a - b; }
-__device__ __forceinline__ double vsub(double a, double b) { return a - b; }
-__device__ __forceinline__ float2 vsub(float2 a, float2 b) {
-  return __fadd2_rn(a, make_float2(-b.x, -b.y));
-}
-__device__ __forceinline__ double2 vsub(double2 a, double2 b) {
-  return make_double2(a.x - b.x, a.y - b.y);
-}
-__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
-__device__ __forceinline__ double vmul(double a, double b) { return a * b; }
-// Scale multiplies stay two scalar __fmul_rn: the packed multiply may be
-// contracted with a following packed add (a unit step right after the scale
-// of a reverse-stepping program) into one fused operation, which rounds
-// differently from the reference's separate multiply and add.
-__device__ __forceinline__ float2 vmul(float2 a, float b) {
-  return make_float2(__fmul_rn(a.x, b), __fmul_rn(a.y, b));
-}
-__device__ __forceinline__ double2 vmul(double2 a, double b) {
-  return make_double2(a.x * b, a.y * b);
-}
-template <typename VT>
-__device__ __forceinline__ VT vzero() {
-  return VT{};
-}
-template <typename T>
-__device__ __forceinline__ T vlane(const T& v, int) { return v; }
-__device__ __forceinline__ float vlane(const float2& v, int k) { return k ? v.y : v.x; }
-__device__ __forceinline__ double vlane(const double2& v, int k) { return k ? v.y : v.x; }
 
 namespace reg {
 
@@ -272,6 +211,7 @@ struct Ctx {
   bool has_l, has_r, line_ok;
   int64_t L, bin, bout, n, e0, tile_lo, tile_hi;
   int buf;
+  int bc;           // boundary condition of the pass
   uint64_t pol_st;  // L2 policy of the band stores
 };
 
@@ -295,7 +235,7 @@ __device__ __forceinline__ VT tap(const VT* xl, const bool* vl, const VT* x,
 // band (nb pairs) may end inside a chunk (lines whose length is not a
 // multiple of the chunk); in-chunk taps past the end are skipped.
 template <typename T, typename VT, int P, int PA, int HMAX, int KIND, int OFF,
-          int NT, int SUB, int HL, int HR, bool EM = false>
+          int NT, int SUB, int HL, int HR, bool EM = false, bool EDGE = false>
 __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
                                        const DevStep<T>& st, Ctx<T>& c,
                                        int64_t gp0, int64_t nb) {
@@ -305,6 +245,14 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
     const int64_t rem = nb - gp0;
     lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
   }
+  // Constant / Symmetric / Reflect: the chunks holding a band end redo
+  // that edge around the Zero update (lw_edge.cuh)
+  constexpr int E = P < edge::kEdge ? P : edge::kEdge;
+  const bool fix = EDGE && !EM && c.bc != BC_ZERO && c.line_ok;
+  const bool efront = fix && gp0 == 0;
+  const bool eback = fix && gp0 + P == nb;
+  VT sf[HL > 0 ? HL : 1], sb[HR > 0 ? HR : 1];
+  const DevProgram<T>& prog = c.p->prog;
   const int nth = c.nth;
   VT* mb = reinterpret_cast<VT*>(c.mb);
   VT* mb_first = mb + (int64_t)((c.buf * 2 + 0) * HMAX) * nth;
@@ -315,6 +263,10 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
   for (int h = 0; h < HL; ++h) mb_last[h * nth + c.tid] = x[P - HL + h];
   __syncthreads();
   c.buf ^= 1;
+  if constexpr (EDGE) {
+    if (efront) edge::call<P, E, false>(st, prog, c.bc, false, y, x, sf, gp0, nb, HL, HR);
+    if (eback) edge::call<P, E, true>(st, prog, c.bc, false, y, x, sb, gp0, nb, HL, HR);
+  }
   VT xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
   bool vl[HL > 0 ? HL : 1], vr[HR > 0 ? HR : 1];
 #pragma unroll
@@ -355,6 +307,10 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
       yi = ok ? f : yi;
     }
     y[i] = yi;
+  }
+  if constexpr (EDGE) {
+    if (efront) edge::call<P, E, false>(st, prog, c.bc, true, y, x, sf, gp0, nb, HL, HR);
+    if (eback) edge::call<P, E, true>(st, prog, c.bc, true, y, x, sb, gp0, nb, HL, HR);
   }
 }
 
@@ -415,10 +371,10 @@ __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
       }
     } else if constexpr (cs.y_is_d) {
       update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
-             cs.right, EM>(d, s, st, c, gp0, nb);
+             cs.right, EM, true>(d, s, st, c, gp0, nb);
     } else {
       update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
-             cs.right, EM>(s, d, st, c, gp0, nb);
+             cs.right, EM, true>(s, d, st, c, gp0, nb);
     }
     steps<T, VT, WI, OP, K + 1, P, PA, HMAX, EM>(s, d, c, gp0, nb);
   }
@@ -668,6 +624,7 @@ __global__ void __launch_bounds__(512)
   c.has_l = c.r > 0;
   c.has_r = c.r < p.tpl - 1;
   c.buf = 0;
+  c.bc = p.bc;
   c.pol_st = l2_store_policy(p.l2hint);
   int64_t tile_idx = 0, group = blockIdx.x;
   if (TILE) {
@@ -724,7 +681,7 @@ __global__ void __launch_bounds__(512)
       if (p.nreg < p.levels) {
         __syncthreads();
         const int64_t m = c.n >> p.nreg;
-        coarse_forward(p.prog, BC_ZERO, c.cA, p.coarse_pitch, c.cB,
+        coarse_forward(p.prog, p.bc, c.cA, p.coarse_pitch, c.cB,
                        p.coarse_pitch_b, lines_cta, m, p.levels - p.nreg);
         // store the coarse region [0, m) of every line of the CTA
         const int64_t tot = (int64_t)lines_cta * m;
@@ -772,7 +729,7 @@ __global__ void __launch_bounds__(512)
           c.cA[(int64_t)jj * p.coarse_pitch + i] = v;
         }
         __syncthreads();
-        coarse_reverse(p.prog, BC_ZERO, c.cA, p.coarse_pitch, c.cB,
+        coarse_reverse(p.prog, p.bc, c.cA, p.coarse_pitch, c.cB,
                        p.coarse_pitch_b, lines_cta, m, p.levels - p.nreg);
       }
     }

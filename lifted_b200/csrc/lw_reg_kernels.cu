@@ -13,6 +13,7 @@
 
 #include "lw_col.hpp"
 #include "lw_col_kernel.cuh"
+#include "lw_edge.cuh"
 #include "lw_launch.hpp"
 #include "lw_reg.hpp"
 #include "lw_reg_inst.hpp"
@@ -88,6 +89,80 @@ bool edges_overlap(const DevProgram<T>& prog, int64_t n, int levels) {
     }
   }
   return false;
+}
+
+// How far from a band end (pairs) the exact edge work of the register
+// kernels reaches under boundary bc (lw_edge.cuh): the largest distance from
+// the nearer end of any element a step's edge loops read or write, on a band
+// long enough that the two ends stay apart.  1 for the Zero boundary (no edge
+// work); -1 when the register kernels do not serve bc (Periodic maps to the
+// far end) or the reach exceeds their edge window.  A launch runs a level in
+// registers only when its chunks hold at least this many pairs.
+template <typename T>
+int edge_footprint(const DevProgram<T>& prog, int bc) {
+  if (bc == BC_ZERO) return 1;
+  if (bc != BC_CONSTANT && bc != BC_SYMMETRIC && bc != BC_REFLECT) return -1;
+  const int64_t nb = (int64_t)1 << 20;
+  int64_t F = 1;
+  auto touch = [&](int64_t idx) {
+    if (idx < 0 || idx >= nb) return;
+    F = std::max<int64_t>(F, idx < nb / 2 ? idx + 1 : nb - idx);
+  };
+  auto taps_at = [&](const DevStep<T>& st, int64_t j, bool mapped) {
+    const int nt = st.kind == K_UNIT ? 1 : st.ntaps;
+    for (int t = 0; t < nt; ++t)
+      touch(mapped ? host_bc_index(bc, j + t, nb) : j + t);
+  };
+  for (int k = 0; k < prog.nsteps; ++k) {
+    const DevStep<T>& st = prog.st[k];
+    if (st.kind == K_SCALE) continue;
+    const int64_t n1 = std::min<int64_t>(st.nf, nb);
+    const int64_t n2 = nb > st.nb ? nb - st.nb : 0;
+    if (prog.normal) {
+      for (int64_t i = 0; i < n1; ++i) {
+        touch(i);
+        taps_at(st, i + st.off, true);
+      }
+      for (int64_t i = n2; i < nb; ++i) {
+        touch(i);
+        taps_at(st, i + st.off, true);
+      }
+      continue;
+    }
+    if (st.kind == K_UNIT) {
+      for (int64_t i = st.fold_off, j = 0; i < 0 && j < nb; ++i, ++j) {
+        const int64_t io = host_bc_index(bc, i, nb);
+        if (io < nb && io != i) {
+          touch(io);
+          touch(j);
+        }
+      }
+    } else {
+      for (int64_t i = st.fold_off, j = 1 - st.ntaps; i < 0; ++i, ++j) {
+        const int64_t io = host_bc_index(bc, i, nb);
+        if (io < nb && io != i) {
+          touch(io);
+          taps_at(st, j, false);
+        }
+      }
+    }
+    for (int64_t i = nb, j = nb + st.off; i < nb - st.off; ++i, ++j) {
+      const int64_t io = host_bc_index(bc, i, nb);
+      if (io < nb && io != i) {
+        touch(io);
+        taps_at(st, j, false);
+      }
+    }
+  }
+  return F > edge::kEdge ? -1 : (int)F;
+}
+
+// Register levels a launch with p0 pairs per chunk at its first level may
+// run under edge footprint F (every level's chunks at least F pairs).
+int edge_levels(int p0, int F) {
+  int l = 0;
+  for (int p = p0; p >= F && p >= 1; p >>= 1) ++l;
+  return l;
 }
 
 // The host-resolved program must have exactly the compile-time structure.
@@ -172,7 +247,9 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   const int64_t n = g.n;
   if (n % (2 * P0)) return 0;
   const int64_t tpl = n / (2 * P0);
-  const int maxreg = reg_max_levels(wi, op, P0);
+  const int F = edge_footprint(*a.prog, a.bc);
+  if (F < 0) return 0;
+  const int maxreg = std::min(reg_max_levels(wi, op, P0), edge_levels(P0, F));
   const int nreg = levels < maxreg ? levels : maxreg;
   if (nreg < 1) return 0;
   int lpc = 1, block;
@@ -202,6 +279,7 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   RegParams<T> p;
   std::memset(&p, 0, sizeof(p));
   p.l2hint = l2_hint_code();
+  p.bc = a.bc;
   p.in = in;
   p.out = out;
   p.g = g;
@@ -357,7 +435,9 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   if (a.in_place) return 0;  // tiles would overwrite other tiles' input
   if (!lines_adjacent(g)) return 0;
   if (n % (2 * P0)) return 0;
-  const int maxreg = reg_max_levels(wi, op, P0);
+  const int F = edge_footprint(*a.prog, a.bc);
+  if (F < 0) return 0;
+  const int maxreg = std::min(reg_max_levels(wi, op, P0), edge_levels(P0, F));
   // choose k so that the approximation band fits a strided whole-line launch
   int k = 0;
   for (int kk = 1; kk <= maxreg && kk <= a.levels; ++kk) {
@@ -401,6 +481,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   RegParams<T> p;
   std::memset(&p, 0, sizeof(p));
   p.l2hint = l2_hint_code();
+  p.bc = a.bc;
   p.g = g;
   p.tmp = tmp;
   p.tmp_line = 1;          // tmp is [position][line]: lines adjacent
@@ -535,9 +616,10 @@ int band_pass(const RegPassArgs<T>& a, const LineGeom& g2, const T* in, T* out, 
 // windows with halos (the smallest k whose band fits whole lines, else the
 // register levels).
 template <typename T>
-bool col_levels_plan(int wi, int op, int64_t n, int levels, int* k_out, int64_t* tile,
+bool col_levels_plan(int wi, int op, int64_t n, int levels, int F, int* k_out, int64_t* tile,
                      int64_t* halo, int64_t* ntr) {
-  const int maxreg = std::min(reg_max_levels(wi, op, COL_P0), COL_MAXK);
+  const int maxreg =
+      std::min({reg_max_levels(wi, op, COL_P0), COL_MAXK, edge_levels(COL_P0, F)});
   int k = 0;
   if (n <= COL_ROWS) {
     k = std::min(levels, maxreg);
@@ -574,18 +656,19 @@ bool col_levels_plan(int wi, int op, int64_t n, int levels, int* k_out, int64_t*
 // for compiled wavelets, ends on the whole-line register kernel.  Checked
 // before the first launch, so no launch is left without its band pass.
 template <typename T>
-bool col_chain_ok(int wi, int op, int64_t n, int levels, int depth) {
+bool col_chain_ok(int wi, int op, int64_t n, int levels, int F, int depth) {
   // lines a multiple of 32 long, or of 2^levels (the band ends inside a
   // chunk: the end-masked instantiation)
   if (depth > 8 || (n % 32 && n % ((int64_t)1 << levels))) return false;
   int k;
   int64_t tile, halo, ntr;
-  if (!col_levels_plan<T>(wi, op, n, levels, &k, &tile, &halo, &ntr)) return false;
+  if (!col_levels_plan<T>(wi, op, n, levels, F, &k, &tile, &halo, &ntr)) return false;
   if (levels == k) return true;
   const int64_t m = n >> k;
-  if (col_chain_ok<T>(wi, op, m, levels - k, depth + 1)) return true;
+  if (col_chain_ok<T>(wi, op, m, levels - k, F, depth + 1)) return true;
   constexpr int P0 = p0_of<T>();
-  return compiled_wavelet(wi) && m % (2 * P0) == 0 && m / (2 * P0) <= 16;
+  return compiled_wavelet(wi) && m % (2 * P0) == 0 && m / (2 * P0) <= 16 &&
+         edge_levels(P0, F) >= 1;
 }
 
 // Strided pass (float32 or float64) on the TMA-staged persistent kernel:
@@ -613,6 +696,9 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // end-masked instantiation, one line per lane
     const bool em = (n % 32) != 0;
     if (em && n % ((int64_t)1 << a.levels)) return 0;
+    // exact band edges of the non-Zero boundaries need whole chunks
+    const int F = edge_footprint(*a.prog, a.bc);
+    if (F < 0 || (em && a.bc != BC_ZERO)) return 0;
     const int wi = a.wi, op = a.op;
     // two adjacent lines per lane (packed FP32x2) when the line groups and
     // every line base of the output stay 8-byte aligned
@@ -623,7 +709,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (n > COL_ROWS && a.in_place) return 0;  // windows would overwrite other windows' input
     int k = 0;
     int64_t tile, halo, ntr;
-    if (!col_levels_plan<T>(wi, op, n, a.levels, &k, &tile, &halo, &ntr)) return 0;
+    if (!col_levels_plan<T>(wi, op, n, a.levels, F, &k, &tile, &halo, &ntr)) return 0;
     const int64_t nouter = g.nother == 2 ? g.oshape[1] : 1;
     // short whole lines of a 3D view: a tile stacks 512/n consecutive outer
     // slices (the staging window stays full)
@@ -653,7 +739,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (!fn) return 0;
     const int64_t m = n >> k;
     const bool more = a.levels > k;
-    if (more && !col_chain_ok<T>(wi, op, n, a.levels, 0)) return 0;
+    if (more && !col_chain_ok<T>(wi, op, n, a.levels, F, 0)) return 0;
     if (!more && a.levels != k) return 0;
     int32_t* err = col_error_flag();
     if (!err) return 0;
@@ -707,6 +793,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     }
     RegParams<T>& r = cp.r;
     r.l2hint = l2_hint_code();
+    r.bc = a.bc;
     r.in = a.in;
     r.out = a.out;
     r.tmp = tmp;
@@ -829,8 +916,14 @@ int check_col_errors(cudaStream_t stream) {
 template <typename T>
 int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
                   RegStats* stats) {
-  if (a.bc != BC_ZERO) return 0;
+  // Zero, and Constant / Symmetric / Reflect with exact band edges on the
+  // kernels built on the register step code (the strided TMA-staged kernel,
+  // the whole-line and tiled register kernels)
+  if (edge_footprint(*a.prog, a.bc) < 0) return 0;
+  const bool zero = a.bc == BC_ZERO;
   if (a.wi < 0 || a.wi >= kNumCatalogue) return 0;
+  // the edge work is compiled into the per-wavelet kernels only
+  if (!zero && !compiled_wavelet(a.wi)) return 0;
   if (a.levels < 1 || a.levels > MAX_LEVELS) return 0;
   if (!structure_matches(*a.prog, a.wi, a.op)) return 0;
   const LineGeom& g = a.g;
@@ -841,6 +934,7 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
     // (float64) samples, strided lines adjacent in memory
     if (!generic_enabled()) return 0;
     if (contiguous) {
+      if (!zero) return 0;
       const int rc = launch_wrow<T>(a, stream, stats);
       if (rc != 0) return rc;
       return launch_wtile<T>(a, stream, stats);
@@ -850,10 +944,13 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
   }
   // whole lines: contiguous rows, or strided lines adjacent in memory
   if (contiguous) {
-    int rc = launch_wrow<T>(a, stream, stats);
-    if (rc != 0) return rc;
-    rc = launch_wtile<T>(a, stream, stats);
-    if (rc != 0) return rc;
+    int rc = 0;
+    if (zero) {
+      rc = launch_wrow<T>(a, stream, stats);
+      if (rc != 0) return rc;
+      rc = launch_wtile<T>(a, stream, stats);
+      if (rc != 0) return rc;
+    }
     rc = launch_whole<T>(a, g, a.in, a.out, a.levels, false, stream, stats);
     if (rc != 0) return rc;
   }
