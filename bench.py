@@ -896,6 +896,28 @@ def main() -> int:
 
     seq = [(0, x, w, 0), (0, w, w, 1), (2, w, y, 0), (2, y, y, 1)]
     mean_launch_ms = device_times([(lambda a=a: launch_axis(*a)) for a in seq])
+    # The same four passes as one-pass graphs replayed back to back after
+    # one L2 flush, events between them: per-pass device times inside the
+    # step (each pass reading what the previous one left in L2).
+    pass_graphs = []
+    for a in seq:
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr, capture_error_mode="thread_local"):
+            launch_axis(*a)
+        pass_graphs.append(gr)
+    in_step = []
+    for k in range(10):
+        flush.fill_(4.0 + k)
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(pass_graphs) + 1)]
+        for i, gr in enumerate(pass_graphs):
+            evs[i].record(stream)
+            gr.replay()
+        evs[-1].record(stream)
+        torch.cuda.synchronize(dev)
+        if k >= 2:
+            in_step.append([evs[i].elapsed_time(evs[i + 1]) for i in range(len(pass_graphs))])
+    in_step_ms = np.median(np.array(in_step), axis=0)
+    del pass_graphs
     eager = []
     for _ in range(5):
         flush.fill_(3.0)
@@ -992,7 +1014,10 @@ def main() -> int:
                                        "forward_adjoint": round(float(col_ms[1]), 4)},
                          "bytes_per_launch": bytes_per_launch,
                          "traffic": traffic,
-                         "per_axis_pass_ms": [round(v, 4) for v in mean_launch_ms.tolist()]},
+                         "per_axis_pass_ms": [round(v, 4) for v in mean_launch_ms.tolist()],
+                         "per_axis_pass_in_step_ms": [round(v, 4) for v in in_step_ms.tolist()],
+                         "passes": "axis 0 Forward, axis 1 Forward, axis 0 ForwardAdjoint, "
+                                   "axis 1 ForwardAdjoint"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),

@@ -10,9 +10,9 @@
 namespace lw {
 namespace {
 
-template <typename T, int WI, int OP, int V, bool EM>
+template <typename T, int WI, int OP, int V, bool EM, bool EDGE>
 cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_t stream) {
-  auto kern = col_kernel<T, WI, OP, V, EM>;
+  auto kern = col_kernel<T, WI, OP, V, EM, EDGE>;
   static bool configured[kMaxDevices] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -27,13 +27,25 @@ cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_
   return launch_overlapped(kern, grid, COL_THREADS, smem, stream, p);
 }
 
-template <typename T, int WI, int V, bool EM>
+template <typename T, int WI, int V, bool EM, bool EDGE = false>
 ColFn<T> by_op(int op) {
   switch (op) {
-    case 0: return launch_one<T, WI, 0, V, EM>;
-    case 1: return launch_one<T, WI, 1, V, EM>;
-    case 2: return launch_one<T, WI, 2, V, EM>;
-    default: return launch_one<T, WI, 3, V, EM>;
+    case 0: return launch_one<T, WI, 0, V, EM, EDGE>;
+    case 1: return launch_one<T, WI, 1, V, EM, EDGE>;
+    case 2: return launch_one<T, WI, 2, V, EM, EDGE>;
+    default: return launch_one<T, WI, 3, V, EM, EDGE>;
+  }
+}
+
+// The compiled wavelets with exact band edges (Constant, Symmetric,
+// Reflect; whole chunks only).
+template <typename T, int V>
+ColFn<T> edge_wavelet(int wi, int op) {
+  switch (wi) {
+    case 2: return by_op<T, 2, V, false, true>(op);
+    case 4: return by_op<T, 4, V, false, true>(op);
+    case 33: return by_op<T, 33, V, false, true>(op);
+    default: return nullptr;
   }
 }
 
@@ -53,12 +65,16 @@ ColFn<T> by_wavelet(int wi, int op) {
 
 }  // namespace
 
-// em: lines whose length is not a multiple of 32 (one line per lane only)
-ColFn<float> pick_col_f32(int wi, int op, int v, bool em) {
+// em: lines whose length is not a multiple of 32 (one line per lane only);
+// edge: the exact-edge instantiation (non-Zero boundaries)
+ColFn<float> pick_col_f32(int wi, int op, int v, bool em, bool edge) {
+  if (edge) return em ? nullptr : (v == 2 ? edge_wavelet<float, 2>(wi, op)
+                                          : edge_wavelet<float, 1>(wi, op));
   if (em) return v == 1 ? by_wavelet<float, 1, true>(wi, op) : nullptr;
   return v == 2 ? by_wavelet<float, 2, false>(wi, op) : by_wavelet<float, 1, false>(wi, op);
 }
-ColFn<double> pick_col_f64(int wi, int op, bool em) {
+ColFn<double> pick_col_f64(int wi, int op, bool em, bool edge) {
+  if (edge) return em ? nullptr : edge_wavelet<double, 1>(wi, op);
   return em ? by_wavelet<double, 1, true>(wi, op) : by_wavelet<double, 1, false>(wi, op);
 }
 

@@ -15,8 +15,10 @@ using ColFn = cudaError_t (*)(const ColParams<T>&, int, size_t, cudaStream_t);
 // Launcher for (catalogue wavelet, transform, lines per lane, lines whose
 // length is not a multiple of 32); nullptr if not compiled.  float64, and
 // such lines, have one line per lane only.
-ColFn<float> pick_col_f32(int wi, int op, int v, bool em);
-ColFn<double> pick_col_f64(int wi, int op, bool em);
+// edge: the instantiation with exact band edges for the Constant, Symmetric
+// and Reflect boundaries (compiled wavelets, whole chunks).
+ColFn<float> pick_col_f32(int wi, int op, int v, bool em, bool edge);
+ColFn<double> pick_col_f64(int wi, int op, bool em, bool edge);
 // Dynamic shared memory of one CTA: staging buffer, mailbox, mbarrier.
 size_t col_smem_bytes(int hmax, int v, int elem_bytes);
 

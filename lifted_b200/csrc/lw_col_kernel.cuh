@@ -27,7 +27,8 @@
 // The lifting arithmetic, the mailbox neighbour exchange and the band
 // stores are those of the register-blocked kernel in tile mode: interior
 // results are exact, the halo absorbs the corrupted window margins,
-// out-of-band taps are skipped (Zero boundary).
+// out-of-band taps are skipped (Zero boundary; the EDGE instantiation redoes
+// the band edges of the Constant, Symmetric and Reflect boundaries).
 #pragma once
 
 #include <cuda.h>
@@ -217,7 +218,7 @@ constexpr bool preload_d1() {
   return sizeof(T) == 4;
 }
 
-template <typename T, int WI, int OP, int P0, int HMAX, int V, int LV, bool EM>
+template <typename T, int WI, int OP, int P0, int HMAX, int V, int LV, bool EM, bool EDGE>
 __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0],
                                            typename LaneVec<T, V>::type (&d)[P0],
                                            const typename LaneVec<T, V>::type (&d1)[P0],
@@ -247,7 +248,7 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
           if (c.tid == 0 && rs.next < rs.p->ntiles)
             issue<T, false, V>(*rs.p, rs.next, const_cast<T*>(rs.stage), rs.bar);
         }
-        reg::steps<T, VT, WI, OP, 0, P, P0, HMAX, EM>(s, d, c, gp0, nb);
+        reg::steps<T, VT, WI, OP, 0, P, P0, HMAX, EM, EDGE>(s, d, c, gp0, nb);
         if constexpr (LV == 0) {
           if (reg::chunk_stored(c)) {
             T* o = p.out + c.bout + c.e0 * p.g.sout;
@@ -270,9 +271,9 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
           }
         }
       }
-      if constexpr (LV > 0) rev_levels<T, WI, OP, P0, HMAX, V, LV - 1, EM>(s, d, d1, c, rs);
+      if constexpr (LV > 0) rev_levels<T, WI, OP, P0, HMAX, V, LV - 1, EM, EDGE>(s, d, d1, c, rs);
     } else if constexpr (LV > 0) {
-      rev_levels<T, WI, OP, P0, HMAX, V, LV - 1, EM>(s, d, d1, c, rs);
+      rev_levels<T, WI, OP, P0, HMAX, V, LV - 1, EM, EDGE>(s, d, d1, c, rs);
     }
   }
 }
@@ -281,7 +282,10 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
 
 // EM: lines whose length is a multiple of 2^levels but not of 32 (the band
 // ends inside a chunk at some level; taps and stores past it are skipped).
-template <typename T, int WI, int OP, int V, bool EM>
+// EDGE: the instantiation for the Constant, Symmetric and Reflect
+// boundaries (exact band edges, lw_edge.cuh); Zero passes run the one
+// without that code.
+template <typename T, int WI, int OP, int V, bool EM, bool EDGE = false>
 __global__ void __launch_bounds__(COL_THREADS, 1)
     col_kernel(const __grid_constant__ ColParams<T> p) {
   using VT = typename LaneVec<T, V>::type;
@@ -369,7 +373,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
       }
       __syncthreads();  // staging consumed
       if (tid == 0 && next < p.ntiles) col::issue<T, FWD, V>(p, next, stage, bar);
-      reg::fwd_levels<T, VT, V, WI, OP, P0, HMAX, 0, true, EM>(s, d, c);
+      reg::fwd_levels<T, VT, V, WI, OP, P0, HMAX, 0, true, EM, EDGE>(s, d, c);
     } else {
       const int k = p.r.nreg;
       VT d1[col::preload_d1<T>() ? P0 : 1];
@@ -384,10 +388,10 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
       col::RevStage<T> rs{stage, bar, &p, next};
       constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
       if constexpr (col::preload_d1<T>()) {
-        col::rev_levels<T, WI, OP, P0, HMAX, V, TOP, EM>(s, d, d1, c, rs);
+        col::rev_levels<T, WI, OP, P0, HMAX, V, TOP, EM, EDGE>(s, d, d1, c, rs);
       } else {
         VT dummy[P0];
-        col::rev_levels<T, WI, OP, P0, HMAX, V, TOP, EM>(s, d, dummy, c, rs);
+        col::rev_levels<T, WI, OP, P0, HMAX, V, TOP, EM, EDGE>(s, d, dummy, c, rs);
       }
     }
   }

@@ -339,7 +339,7 @@ __device__ __forceinline__ void gen_update(int shape, VT (&s)[PA], VT (&d)[PA],
 }
 
 template <typename T, typename VT, int WI, int OP, int K, int P, int PA,
-          int HMAX, bool EM = false>
+          int HMAX, bool EM = false, bool EDGE = false>
 __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
                                       int64_t gp0, int64_t nb) {
   if constexpr (is_gen(WI)) {
@@ -371,12 +371,12 @@ __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
       }
     } else if constexpr (cs.y_is_d) {
       update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
-             cs.right, EM, true>(d, s, st, c, gp0, nb);
+             cs.right, EM, EDGE>(d, s, st, c, gp0, nb);
     } else {
       update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
-             cs.right, EM, true>(s, d, st, c, gp0, nb);
+             cs.right, EM, EDGE>(s, d, st, c, gp0, nb);
     }
-    steps<T, VT, WI, OP, K + 1, P, PA, HMAX, EM>(s, d, c, gp0, nb);
+    steps<T, VT, WI, OP, K + 1, P, PA, HMAX, EM, EDGE>(s, d, c, gp0, nb);
   }
 }
 
@@ -428,7 +428,7 @@ __device__ __forceinline__ bool chunk_stored(const Ctx<T>& c) {
 // EM: lines whose length is a multiple of 2^levels but not of the chunk;
 // the band ends inside a chunk, whose stores stop there.
 template <typename T, typename VT, int V, int WI, int OP, int P0, int HMAX,
-          int LV, bool TILE, bool EM = false>
+          int LV, bool TILE, bool EM = false, bool EDGE = false>
 __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
                                            Ctx<T>& c) {
   constexpr int P = P0 >> LV;
@@ -441,7 +441,7 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
         const int64_t rem = nb - gp0;
         lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
       }
-      steps<T, VT, WI, OP, 0, P, P0, HMAX, EM>(s, d, c, gp0, nb);
+      steps<T, VT, WI, OP, 0, P, P0, HMAX, EM, EDGE>(s, d, c, gp0, nb);
       if (chunk_stored(c)) {
         if constexpr (EM) store_first<T, VT, P, P0>(d, c, nb + gp0, lim);
         else store_run<T, VT, P, P0>(d, c, nb + gp0);
@@ -480,7 +480,7 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
         d[i] = s[2 * i + 1];
         s[i] = s[2 * i];
       }
-      fwd_levels<T, VT, V, WI, OP, P0, HMAX, LV + 1, TILE, EM>(s, d, c);
+      fwd_levels<T, VT, V, WI, OP, P0, HMAX, LV + 1, TILE, EM, EDGE>(s, d, c);
     }
   }
 }
@@ -488,7 +488,7 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
 // Reverse-stepping register levels (Inverse, ForwardAdjoint), coarsest
 // register level first.
 template <typename T, typename VT, int V, int WI, int OP, int P0, int HMAX,
-          int LV, bool TILE>
+          int LV, bool TILE, bool EDGE = false>
 __device__ __forceinline__ void rev_levels(VT (&s)[P0], VT (&d)[P0],
                                            Ctx<T>& c) {
   constexpr int P = P0 >> LV;
@@ -535,7 +535,7 @@ __device__ __forceinline__ void rev_levels(VT (&s)[P0], VT (&d)[P0],
                      ? *reinterpret_cast<const VT*>(p.in + c.bin + (nb + q) * p.g.sin)
                      : vzero<VT>();
         }
-        steps<T, VT, WI, OP, 0, P, P0, HMAX>(s, d, c, gp0, nb);
+        steps<T, VT, WI, OP, 0, P, P0, HMAX, false, EDGE>(s, d, c, gp0, nb);
         if constexpr (LV == 0) {
           if (chunk_stored(c)) {
             T* o = p.out + c.bout + c.e0 * p.g.sout;
@@ -569,9 +569,9 @@ __device__ __forceinline__ void rev_levels(VT (&s)[P0], VT (&d)[P0],
         }
       }
       if constexpr (LV > 0)
-        rev_levels<T, VT, V, WI, OP, P0, HMAX, LV - 1, TILE>(s, d, c);
+        rev_levels<T, VT, V, WI, OP, P0, HMAX, LV - 1, TILE, EDGE>(s, d, c);
     } else if constexpr (LV > 0) {
-      rev_levels<T, VT, V, WI, OP, P0, HMAX, LV - 1, TILE>(s, d, c);
+      rev_levels<T, VT, V, WI, OP, P0, HMAX, LV - 1, TILE, EDGE>(s, d, c);
     }
   }
 }
@@ -588,7 +588,10 @@ constexpr int reg_max_levels(int wi, int op, int p0) {
 
 // V: adjacent lines per lane (strided mode only; 2 packs float pairs into
 // FP32x2 arithmetic and 8-byte accesses).  lines per CTA = lpc * V.
-template <typename T, int WI, int OP, int P0, bool STRIDED, bool TILE, int V>
+// EDGE: the instantiation for the Constant, Symmetric and Reflect
+// boundaries (exact band edges, lw_edge.cuh); Zero passes run the one
+// without that code.
+template <typename T, int WI, int OP, int P0, bool STRIDED, bool TILE, int V, bool EDGE = false>
 __global__ void __launch_bounds__(512)
     reg_kernel(const __grid_constant__ RegParams<T> p) {
   using VT = typename LaneVec<T, V>::type;
@@ -676,7 +679,7 @@ __global__ void __launch_bounds__(512)
                        : vzero<VT>();
       }
     }
-    reg::fwd_levels<T, VT, V, WI, OP, P0, HMAX, 0, TILE>(s, d, c);
+    reg::fwd_levels<T, VT, V, WI, OP, P0, HMAX, 0, TILE, false, EDGE>(s, d, c);
     if constexpr (!TILE) {
       if (p.nreg < p.levels) {
         __syncthreads();
@@ -734,7 +737,7 @@ __global__ void __launch_bounds__(512)
       }
     }
     constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
-    reg::rev_levels<T, VT, V, WI, OP, P0, HMAX, TOP, TILE>(s, d, c);
+    reg::rev_levels<T, VT, V, WI, OP, P0, HMAX, TOP, TILE, EDGE>(s, d, c);
   }
 }
 

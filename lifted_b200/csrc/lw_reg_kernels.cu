@@ -37,11 +37,11 @@ constexpr int p0_of() {
 }
 
 template <typename T>
-RegFn<T> pick(int wi, int op, bool strided, bool tile, int v) {
+RegFn<T> pick(int wi, int op, bool strided, bool tile, int v, bool edge) {
   if constexpr (sizeof(T) == 4)
-    return pick_reg_f32(wi, op, strided, tile, v);
+    return pick_reg_f32(wi, op, strided, tile, v, edge);
   else
-    return pick_reg_f64(wi, op, strided, tile, v);
+    return pick_reg_f64(wi, op, strided, tile, v, edge);
 }
 
 bool compiled_wavelet(int wi) {
@@ -293,7 +293,7 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   p.prog = *a.prog;
   const int64_t groups = (g.nlines + lines_cta - 1) / lines_cta;
   if (groups > 0x7fffffffLL) return 0;
-  RegFn<T> fn = pick<T>(wi, op, strided, false, v);
+  RegFn<T> fn = pick<T>(wi, op, strided, false, v, a.bc != BC_ZERO);
   if (!fn) return 0;
   cudaError_t e = fn(p, (int)groups, block, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
@@ -494,7 +494,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   p.halo = halo;
   p.ntiles = ntiles;
   p.prog = *a.prog;
-  RegFn<T> tfn = pick<T>(wi, op, true, true, v);
+  RegFn<T> tfn = pick<T>(wi, op, true, true, v, a.bc != BC_ZERO);
   if (!tfn) {
     if (tmp) scratch_free(tmp, stream);
     return 0;
@@ -734,8 +734,8 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     const int wk = wide ? WI_GENW : (gen ? WI_GEN : wi);
     ColFn<T> fn;
     if (em) v = 1;
-    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v, em);
-    else fn = pick_col_f64(wk, op, em);
+    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v, em, a.bc != BC_ZERO);
+    else fn = pick_col_f64(wk, op, em, a.bc != BC_ZERO);
     if (!fn) return 0;
     const int64_t m = n >> k;
     const bool more = a.levels > k;
