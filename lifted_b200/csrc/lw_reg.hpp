@@ -48,8 +48,6 @@ bool col_stacked();
 // Whether its tiles run in row-tile-major order (the "col_row_order"
 // option).
 bool col_row_order();
-// The "tma_l2_promotion" option (0..3).
-int tma_promotion_option();
 // Synchronises `stream`; returns 1 (and clears it) if a TMA-staged kernel
 // gave up waiting for a staging copy since the last check, 0 if not, -1 if
 // the check itself failed.

@@ -322,10 +322,9 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       p.levels = a.levels;
       p.l2hint = l2_hint_code();
       p.prog = *a.prog;
-      const size_t smem = wrow2_smem((int)q0);
-      const int64_t grid =
-          std::min<int64_t>((g.nlines + 1) / 2,
-                            (int64_t)sm_count() * wrow2_resident_ctas(a.wi, a.op, (int)q0));
+      const size_t smem = (size_t)4 * (size_t)g.n * sizeof(T);
+      const int64_t grid = std::min<int64_t>((g.nlines + 1) / 2,
+                                             (int64_t)sm_count() * wrow2_resident_ctas((int)q0));
       if (grid <= 0x7fffffffLL) {
         cudaError_t e = launch_wrow2_f32(a.wi, a.op, (int)q0, p, (int)grid, smem, stream);
         if (e != cudaSuccess) return -(int)e - 1000;
@@ -553,17 +552,6 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   return rc;
 }
 
-// L2 promotion of the TMA boxes (the "tma_l2_promotion" option: 0 none,
-// 1 64 B, 2 128 B, 3 256 B).
-CUtensorMapL2promotion tma_l2_promotion() {
-  switch (tma_promotion_option()) {
-    case 0: return CU_TENSOR_MAP_L2_PROMOTION_NONE;
-    case 1: return CU_TENSOR_MAP_L2_PROMOTION_L2_64B;
-    case 3: return CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
-    default: return CU_TENSOR_MAP_L2_PROMOTION_L2_128B;
-  }
-}
-
 // Device word the TMA-staged kernel sets when a staging wait gives up.
 int32_t* col_error_flag() {
   static int32_t* flag[kMaxDevices] = {};
@@ -615,7 +603,7 @@ bool encode_rows(CUtensorMap* m, const void* base, int rank, const cuuint64_t* d
   return enc(m, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
              (cuuint32_t)rank, const_cast<void*>(base),
              dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-             tma_l2_promotion(), CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <typename T>

@@ -25,15 +25,11 @@ cudaError_t launch_wrow_f64(int wi, int op, int p0, const WRowParams<double>& p,
 int wrow2_levels_f32(int wi, int op, int p0);
 cudaError_t launch_wrow2_f32(int wi, int op, int p0, const WRowParams<float>& p, int grid,
                              size_t smem, cudaStream_t stream);
-// CTAs per SM of the two-warp kernel (grid sizing of the persistent
-// launch) and its dynamic shared memory.
-int wrow2_resident_ctas(int wi, int op, int p0);
-size_t wrow2_smem(int p0);
+// CTAs per SM the two-warp kernel's shared memory allows (grid sizing of
+// the persistent launch).
+int wrow2_resident_ctas(int p0);
 // Whether contiguous float32 rows may use it (the "wrow_split" option).
 bool wrow2_enabled();
-// Whether it stores its bands straight from registers with one row buffer
-// per slot (the "wrow2_direct" option), else through shared memory.
-bool wrow2_direct();
 
 // Windowed rows (rows longer than one warp holds): pairs per lane of the
 // window (32 for float32, 16 for float64), levels compiled for (catalogue

@@ -189,166 +189,7 @@ __device__ __forceinline__ void rev(float (&s)[P0], float (&d)[P0], float* buf,
   }
 }
 
-// P consecutive values of a lane run stored straight to global memory at
-// element e of the row (e a multiple of P: 16-byte stores for P >= 4).
-template <int P, int PA>
-__device__ __forceinline__ void gstore(float* row, int e, const float (&v)[PA], uint64_t pol) {
-  float* q = row + e;
-  if constexpr (P >= 4) {
-#pragma unroll
-    for (int i = 0; i < P; i += 4) st_hint(q + i, make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]), pol);
-  } else if constexpr (P == 2) {
-    st_hint(q, make_float2(v[0], v[1]), pol);
-  } else {
-    st_hint(q, v[0], pol);
-  }
-}
-
-// Forward levels of the direct-store kernel: every detail band and the last
-// approximation band go from the registers straight to the output row.
-template <int WI, int OP, int P0, int HMAX, int LV>
-__device__ __forceinline__ void fwd_ds(float (&s)[P0], float (&d)[P0], float* row,
-                                       const DevProgram<float>& prog, int levels, Seam& sm,
-                                       uint64_t pol) {
-  constexpr int P = P0 >> LV;
-  if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
-    if (LV < levels) {
-      constexpr int NB = GL * P;
-      const int g = sm.half * 32 + sm.lane;
-      steps<WI, OP, 0, P, P0, HMAX>(s, d, prog, sm);
-      gstore<P>(row, NB + P * g, d, pol);
-      if (LV + 1 == levels) {
-        gstore<P>(row, P * g, s, pol);
-        return;
-      }
-#pragma unroll
-      for (int i = 0; i < P / 2; ++i) {
-        d[i] = s[2 * i + 1];
-        s[i] = s[2 * i];
-      }
-      fwd_ds<WI, OP, P0, HMAX, LV + 1>(s, d, row, prog, levels, sm, pol);
-    }
-  }
-}
-
-// Reverse levels of the direct-store kernel: as rev(), and once the finest
-// band has been read the row buffer is free, so `done` runs (the next row's
-// copy starts) before the last level's steps.
-template <int WI, int OP, int P0, int HMAX, int LV, typename F>
-__device__ __forceinline__ void rev_ds(float (&s)[P0], float (&d)[P0], const float* buf,
-                                       const DevProgram<float>& prog, int levels, Seam& sm,
-                                       F& done) {
-  constexpr int P = P0 >> LV;
-  if constexpr (LV >= 0) {
-    if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
-      if (LV < levels) {
-        constexpr int NB = GL * P;
-        const int g = sm.half * 32 + sm.lane;
-        if (LV + 1 == levels) wrow::read_run<float, P, P>(const_cast<float*>(buf), P * g, s);
-        wrow::read_run<float, P, P>(const_cast<float*>(buf), NB + P * g, d);
-        if constexpr (LV == 0) done();
-        steps<WI, OP, 0, P, P0, HMAX>(s, d, prog, sm);
-        if constexpr (LV > 0) {
-#pragma unroll
-          for (int i = P - 1; i >= 0; --i) {
-            s[2 * i + 1] = d[i];
-            s[2 * i] = s[i];
-          }
-        }
-      }
-    }
-    if constexpr (LV > 0) rev_ds<WI, OP, P0, HMAX, LV - 1>(s, d, buf, prog, levels, sm, done);
-  }
-}
-
 }  // namespace wrow2
-
-// The direct-store form of the two-warp kernel: one row buffer per row slot,
-// used for the row's input only.  Forward: the row is copied in, moved to
-// registers, and the buffer takes the next row's copy at once while the
-// levels run and every band is stored from the registers (a lane's band runs
-// are contiguous in the output, 16-byte stores).  Reverse: the bands are
-// copied into the buffer in the banded layout, read level by level, and the
-// next row's copy starts once the finest band is read; the finished row goes
-// from the registers to the output (a lane's 2 * P0 samples, contiguous).
-// Half the shared memory of the staged form, so more row slots fit an SM.
-template <int WI, int OP, int P0>
-__global__ void __launch_bounds__(128)
-    wrow2d_kernel(const __grid_constant__ WRowParams<float> p) {
-  constexpr int N = 128 * P0;     // row length
-  constexpr int UNITS = N / 4;    // 16-byte units per row
-  constexpr int HMAX = cat_reach(WI, OP) > 0 ? cat_reach(WI, OP) : 1;
-  constexpr bool FWD = (OP == TF_F || OP == TF_IA);
-  extern __shared__ __align__(16) unsigned char lw_wrow2_smem[];
-  __shared__ float mbox[2][2 * 2 * HMAX];
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int rsel = warp >> 1;            // row slot of the CTA
-  const int half = warp & 1;
-  const int t64 = threadIdx.x & 63;      // thread within the slot
-  float* buf = reinterpret_cast<float*>(lw_wrow2_smem) + (int64_t)rsel * N;
-  wrow2::Seam sm{mbox[rsel], half, lane, 1 + rsel, 0};
-  const int nbl = N >> p.levels;
-  constexpr int SHA = wrow::swz_shift_bytes(2 * P0 * 4);
-  const int g = half * 32 + lane;
-  const int64_t step = (int64_t)gridDim.x * 2;
-  const uint64_t pol_ld = l2_load_policy(p.l2hint);
-  const uint64_t pol_st = l2_store_policy(p.l2hint);
-
-  auto load = [&](int64_t row) {
-    int64_t bin, bout;
-    line_base(p.g, row, bin, bout);
-    const float* src = p.in + bin;
-#pragma unroll 4
-    for (int u = t64; u < UNITS; u += 64) {
-      const int sh = FWD ? SHA : wrow2::banded_shift(u, nbl);
-      const unsigned saddr = (unsigned)__cvta_generic_to_shared(buf + wrow::swz(u, sh) * 4);
-      cp_async16_hint(saddr, src + (int64_t)u * 4, pol_ld);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  };
-
-  int64_t row = (int64_t)blockIdx.x * 2 + rsel;
-  pdl_wait();  // the previous kernel's results (no global access before)
-  if (row < p.g.nlines) load(row);
-  for (; row < p.g.nlines; row += step) {
-    const int64_t next = row + step;
-    if (next >= p.g.nlines) pdl_trigger();  // the slot's last row
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // this row's copy
-    wrow2::row_sync(sm.bar_id);
-    int64_t bin, bout;
-    line_base(p.g, row, bin, bout);
-    float* dst = p.out + bout;
-    // the buffer is read: every thread of the slot is past its reads
-    auto done = [&]() {
-      wrow2::row_sync(sm.bar_id);
-      if (next < p.g.nlines) load(next);
-    };
-    float s[P0], d[P0];
-    if constexpr (FWD) {
-      float x[2 * P0];
-      wrow::read_run<float, 2 * P0, 2 * P0>(buf, 2 * P0 * g, x);
-#pragma unroll
-      for (int i = 0; i < P0; ++i) {
-        s[i] = x[2 * i];
-        d[i] = x[2 * i + 1];
-      }
-      done();
-      wrow2::fwd_ds<WI, OP, P0, HMAX, 0>(s, d, dst, p.prog, p.levels, sm, pol_st);
-    } else {
-      constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
-      wrow2::rev_ds<WI, OP, P0, HMAX, TOP>(s, d, buf, p.prog, p.levels, sm, done);
-      float x[2 * P0];
-#pragma unroll
-      for (int i = 0; i < P0; ++i) {
-        x[2 * i] = s[i];
-        x[2 * i + 1] = d[i];
-      }
-      wrow2::gstore<2 * P0>(dst, 2 * P0 * g, x, pol_st);
-    }
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
 
 // 128 threads = two row slots of 128 * P0 float32 elements, two warps each.
 // Persistent: each slot walks rows blockIdx.x*2 + slot, + 2*gridDim.x, ...
