@@ -310,9 +310,13 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   // catalogue wavelets without a compiled kernel: the generic instantiation,
   // every register level the wavelet's reach allows (no compacted levels)
   const bool gen = !compiled_wavelet(a.wi);
+  // Constant / Symmetric / Reflect: the one-warp kernel's exact-edge
+  // instantiation, compiled wavelets only
+  const bool zero = a.bc == BC_ZERO;
+  if (!zero && gen) return 0;
   if constexpr (sizeof(T) == 4) {
     const int64_t q0 = g.n / 128;
-    if (!gen && wrow2_enabled() && g.n % 128 == 0 && (q0 == 16 || q0 == 32) &&
+    if (zero && !gen && wrow2_enabled() && g.n % 128 == 0 && (q0 == 16 || q0 == 32) &&
         wrow2_levels_f32(a.wi, a.op, (int)q0) >= a.levels) {
       WRowParams<T> p;
       std::memset(&p, 0, sizeof(p));
@@ -349,12 +353,28 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     lv = sizeof(T) == 4 ? wrow_levels_f32(a.wi, a.op, (int)p0) : wrow_levels_f64(a.wi, a.op, (int)p0);
   }
   if (lc < 0 || lv < a.levels || (gen && lc < 1)) return 0;
+  if (!zero) {
+    // every level's lanes must hold the edge work's reach: the register
+    // levels' pairs, then the compacted lanes' pairs
+    const int F = edge_footprint(*a.prog, a.bc);
+    if (F < 0) return 0;
+    const int lreg = reg_max_levels(a.wi, a.op, (int)p0);
+    for (int j = 0; j < std::min(lreg, a.levels); ++j)
+      if (((int)p0 >> j) < F) return 0;
+    if (a.levels > lreg) {
+      const int reach = std::max(cat_reach(a.wi, a.op), 1);
+      int pc = 1;
+      while (pc < reach) pc <<= 1;
+      if (pc < F) return 0;
+    }
+  }
   WRowParams<T> p;
   std::memset(&p, 0, sizeof(p));
   p.in = a.in;
   p.out = a.out;
   p.g = g;
   p.levels = a.levels;
+  p.bc = a.bc;
   p.prog = *a.prog;
   if (gen && !set_gen_shapes(&p.prog, a.op)) return 0;
   p.reg_levels = lc;
@@ -366,9 +386,9 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   if (grid > 0x7fffffffLL) return 0;
   cudaError_t e;
   if constexpr (sizeof(T) == 4)
-    e = launch_wrow_f32(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
+    e = launch_wrow_f32(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream, !zero);
   else
-    e = launch_wrow_f64(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream);
+    e = launch_wrow_f64(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream, !zero);
   if (e != cudaSuccess) return -(int)e - 1000;
   counted(stats, KF_WROW);
   return 1;
@@ -944,10 +964,9 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
   }
   // whole lines: contiguous rows, or strided lines adjacent in memory
   if (contiguous) {
-    int rc = 0;
+    int rc = launch_wrow<T>(a, stream, stats);
+    if (rc != 0) return rc;
     if (zero) {
-      rc = launch_wrow<T>(a, stream, stats);
-      if (rc != 0) return rc;
       rc = launch_wtile<T>(a, stream, stats);
       if (rc != 0) return rc;
     }

@@ -15,10 +15,12 @@ struct WRowParams;
 int wrow_levels_f32(int wi, int op, int p0);
 int wrow_levels_f64(int wi, int op, int p0);
 
+// edge: the exact-edge instantiation (Constant, Symmetric, Reflect;
+// compiled wavelets).
 cudaError_t launch_wrow_f32(int wi, int op, int p0, const WRowParams<float>& p,
-                            int grid, int block, size_t smem, cudaStream_t stream);
+                            int grid, int block, size_t smem, cudaStream_t stream, bool edge);
 cudaError_t launch_wrow_f64(int wi, int op, int p0, const WRowParams<double>& p,
-                            int grid, int block, size_t smem, cudaStream_t stream);
+                            int grid, int block, size_t smem, cudaStream_t stream, bool edge);
 
 // Two warps per row (float32 rows of 128 * p0 elements, p0 16 or 32; 128
 // threads = two rows per CTA): levels compiled, 0 if none; launcher.

@@ -10,10 +10,10 @@ namespace lw {
 
 namespace {
 
-template <int WI, int OP, int P0>
+template <int WI, int OP, int P0, bool EDGE>
 cudaError_t launch_one(const WRowParams<float>& p, int grid, int block,
                        size_t smem, cudaStream_t stream) {
-  auto kern = wrow_kernel<float, WI, OP, P0>;
+  auto kern = wrow_kernel<float, WI, OP, P0, EDGE>;
   static bool configured[kMaxDevices] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -30,13 +30,13 @@ cudaError_t launch_one(const WRowParams<float>& p, int grid, int block,
 
 using Fn = cudaError_t (*)(const WRowParams<float>&, int, int, size_t, cudaStream_t);
 
-template <int WI, int P0>
+template <int WI, int P0, bool EDGE = false>
 Fn by_op(int op) {
   switch (op) {
-    case 0: return launch_one<WI, 0, P0>;
-    case 1: return launch_one<WI, 1, P0>;
-    case 2: return launch_one<WI, 2, P0>;
-    default: return launch_one<WI, 3, P0>;
+    case 0: return launch_one<WI, 0, P0, EDGE>;
+    case 1: return launch_one<WI, 1, P0, EDGE>;
+    case 2: return launch_one<WI, 2, P0, EDGE>;
+    default: return launch_one<WI, 3, P0, EDGE>;
   }
 }
 
@@ -47,6 +47,18 @@ Fn by_wavelet(int wi, int op) {
     case 4: return by_op<4, P0>(op);
     case 33: return by_op<33, P0>(op);
     case WI_GEN: return by_op<WI_GEN, P0>(op);
+    default: return nullptr;
+  }
+}
+
+// The exact-edge instantiations (Constant, Symmetric, Reflect) of the
+// compiled wavelets.
+template <int P0>
+Fn edge_wavelet(int wi, int op) {
+  switch (wi) {
+    case 2: return by_op<2, P0, true>(op);
+    case 4: return by_op<4, P0, true>(op);
+    case 33: return by_op<33, P0, true>(op);
     default: return nullptr;
   }
 }
@@ -65,13 +77,13 @@ int wrow_levels_f32(int wi, int op, int p0) {
 
 cudaError_t launch_wrow_f32(int wi, int op, int p0, const WRowParams<float>& p,
                             int grid, int block, size_t smem,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, bool edge) {
   Fn fn = nullptr;
   switch (p0) {
-    case 8: fn = by_wavelet<8>(wi, op); break;
-    case 16: fn = by_wavelet<16>(wi, op); break;
-    case 32: fn = by_wavelet<32>(wi, op); break;
-    case 64: fn = by_wavelet<64>(wi, op); break;
+    case 8: fn = edge ? edge_wavelet<8>(wi, op) : by_wavelet<8>(wi, op); break;
+    case 16: fn = edge ? edge_wavelet<16>(wi, op) : by_wavelet<16>(wi, op); break;
+    case 32: fn = edge ? edge_wavelet<32>(wi, op) : by_wavelet<32>(wi, op); break;
+    case 64: fn = edge ? edge_wavelet<64>(wi, op) : by_wavelet<64>(wi, op); break;
     default: break;
   }
   if (!fn) return cudaErrorInvalidValue;

@@ -24,6 +24,7 @@
 
 #include <cstdint>
 
+#include "lw_edge.cuh"
 #include "lw_reg_kernel.cuh"
 
 namespace lw {
@@ -37,7 +38,8 @@ struct WRowParams {
   int32_t reg_levels;  // generic instantiation: levels in registers (the
                        // rest on compacted lanes); unused otherwise
   int32_t l2hint;      // two-warp kernel: L2 priorities (lw_cache.cuh)
-  int32_t pad_;
+  int32_t bc;          // boundary: Zero, or Constant / Symmetric / Reflect
+                       // in the warp-per-row kernel's EDGE instantiation
   DevProgram<T> prog;
 };
 
@@ -125,6 +127,16 @@ __device__ __forceinline__ void write_run(T* buf, int e, const T (&v)[PA]) {
   }
 }
 
+// What a lane at a band end needs for the exact edges of the Constant,
+// Symmetric and Reflect boundaries (lw_edge.cuh): the program, the
+// boundary and the band's length in pairs.
+template <typename T>
+struct WEdge {
+  const DevProgram<T>* prog;
+  int bc;
+  int64_t nb;
+};
+
 // One step over the lane's P pairs; halos by shuffle.  okl / okr: the
 // left / right neighbour lane holds pairs of the same band (whole rows:
 // lane > 0 / lane < the last active lane; windows: also by band position).
@@ -132,17 +144,32 @@ __device__ __forceinline__ void write_run(T* buf, int e, const T (&v)[PA]) {
 // inside its right neighbour, after that lane's first `rlim` pairs (windows
 // of rows whose length is not a multiple of the lane's pairs); taps past
 // the end are skipped like taps past the band edge.
+// EDGE: whole rows only (okl false exactly at the band's first lane, okr
+// false at its last); the lanes at the band ends redo their edge around the
+// Zero update when the boundary is not Zero (ed).
 template <typename T, int P, int PA, int KIND, int OFF, int NT, int SUB,
-          int HL, int HR, bool EM = false>
+          int HL, int HR, bool EM = false, bool EDGE = false>
 __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
                                         const DevStep<T>& st, bool okl, bool okr,
-                                        int lim = P, int rlim = P) {
+                                        int lim = P, int rlim = P,
+                                        const WEdge<T>* ed = nullptr) {
   static_assert(HL <= P && HR <= P, "step reaches past the neighbour lane");
   T xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
 #pragma unroll
   for (int h = 0; h < HL; ++h) xl[h] = __shfl_up_sync(FULL, x[P - HL + h], 1);
 #pragma unroll
   for (int h = 0; h < HR; ++h) xr[h] = __shfl_down_sync(FULL, x[h], 1);
+  constexpr int E = P < edge::kEdge ? P : edge::kEdge;
+  T sf[HL > 0 ? HL : 1], sb[HR > 0 ? HR : 1];
+  bool efront = false, eback = false;
+  if constexpr (EDGE) {
+    efront = ed->bc != BC_ZERO && !okl;
+    eback = ed->bc != BC_ZERO && !okr;
+    if (efront)
+      edge::call<P, E, false>(st, *ed->prog, ed->bc, false, y, x, sf, 0, ed->nb, HL, HR);
+    if (eback)
+      edge::call<P, E, true>(st, *ed->prog, ed->bc, false, y, x, sb, ed->nb - P, ed->nb, HL, HR);
+  }
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     T yi = y[i];
@@ -177,6 +204,12 @@ __device__ __forceinline__ void wupdate(T (&y)[PA], const T (&x)[PA],
     }
     y[i] = yi;
   }
+  if constexpr (EDGE) {
+    if (efront)
+      edge::call<P, E, false>(st, *ed->prog, ed->bc, true, y, x, sf, 0, ed->nb, HL, HR);
+    if (eback)
+      edge::call<P, E, true>(st, *ed->prog, ed->bc, true, y, x, sb, ed->nb - P, ed->nb, HL, HR);
+  }
 }
 
 // Generic kernels: the update of one step, dispatched on its shape index
@@ -203,10 +236,11 @@ __device__ __forceinline__ void wgen_update(int shape, T (&s)[PA], T (&d)[PA],
   }
 }
 
-template <typename T, int WI, int OP, int K, int P, int PA, bool EM = false>
+template <typename T, int WI, int OP, int K, int P, int PA, bool EM = false, bool EDGE = false>
 __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
                                        const DevProgram<T>& prog, bool okl, bool okr,
-                                       int lim = P, int rlim = P) {
+                                       int lim = P, int rlim = P,
+                                       const WEdge<T>* ed = nullptr) {
   if constexpr (WI == WI_GEN) {
     if constexpr (K == 0) {
       for (int k = 0; k < prog.nsteps; ++k) {
@@ -234,13 +268,13 @@ __device__ __forceinline__ void wsteps(T (&s)[PA], T (&d)[PA],
         d[i] = d[i] * dm;
       }
     } else if constexpr (cs.y_is_d) {
-      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(d, s, st, okl,
-                                                                                okr, lim, rlim);
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM, EDGE>(
+          d, s, st, okl, okr, lim, rlim, ed);
     } else {
-      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(s, d, st, okl,
-                                                                                okr, lim, rlim);
+      wupdate<T, P, PA, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM, EDGE>(
+          s, d, st, okl, okr, lim, rlim, ed);
     }
-    wsteps<T, WI, OP, K + 1, P, PA, EM>(s, d, prog, okl, okr, lim, rlim);
+    wsteps<T, WI, OP, K + 1, P, PA, EM, EDGE>(s, d, prog, okl, okr, lim, rlim, ed);
   }
 }
 
@@ -283,9 +317,9 @@ __device__ __forceinline__ void take_pairs(T* buf, int lane, int act, T (&cs)[PC
 
 // Forward levels lv0 .. levels-1 on a band whose approximation a_lv0 is
 // in s, P elements per lane (32 * P elements).
-template <typename T, int WI, int OP, int P, int PA>
+template <typename T, int WI, int OP, int P, int PA, bool EDGE = false>
 __device__ __forceinline__ void wcompact_fwd(const T (&s)[PA], T* buf, const DevProgram<T>& prog,
-                                             int levels, int lv0, int lane) {
+                                             int levels, int lv0, int lane, int bc = BC_ZERO) {
   constexpr int PC = compact_pairs<WI, OP>();
   static_assert(16 * P >= PC, "band too short to compact");
   write_run<T, P, P>(buf, P * lane, s);
@@ -296,7 +330,9 @@ __device__ __forceinline__ void wcompact_fwd(const T (&s)[PA], T* buf, const Dev
   __syncwarp();
   for (int lv = lv0; lv < levels; ++lv) {
     const int nb = act * PC;  // pairs of this level's band
-    wsteps<T, WI, OP, 0, PC, PC>(cs, cd, prog, lane > 0, lane < act - 1);
+    const WEdge<T> ed{&prog, bc, nb};
+    wsteps<T, WI, OP, 0, PC, PC, false, EDGE>(cs, cd, prog, lane > 0, lane < act - 1, PC, PC,
+                                              &ed);
     if (lane < act) write_run<T, 1, PC>(buf, nb + PC * lane, cd);
     if (lane < act) write_run<T, 1, PC>(buf, PC * lane, cs);
     if (lv + 1 == levels) return;
@@ -309,9 +345,9 @@ __device__ __forceinline__ void wcompact_fwd(const T (&s)[PA], T* buf, const Dev
 
 // Reverse levels levels-1 .. lv0 (coarsest first); leaves a_lv0 in s, P
 // elements per lane, for the register levels below.
-template <typename T, int WI, int OP, int P, int PA>
+template <typename T, int WI, int OP, int P, int PA, bool EDGE = false>
 __device__ __forceinline__ void wcompact_rev(T (&s)[PA], T* buf, const DevProgram<T>& prog,
-                                             int levels, int lv0, int lane) {
+                                             int levels, int lv0, int lane, int bc = BC_ZERO) {
   constexpr int PC = compact_pairs<WI, OP>();
   static_assert(16 * P >= PC, "band too short to compact");
   int act = ((16 * P) >> (levels - 1 - lv0)) / PC;
@@ -330,7 +366,9 @@ __device__ __forceinline__ void wcompact_rev(T (&s)[PA], T* buf, const DevProgra
 #pragma unroll
       for (int i = 0; i < PC; ++i) cd[i] = T(0);
     }
-    wsteps<T, WI, OP, 0, PC, PC>(cs, cd, prog, lane > 0, lane < act - 1);
+    const WEdge<T> ed{&prog, bc, nb};
+    wsteps<T, WI, OP, 0, PC, PC, false, EDGE>(cs, cd, prog, lane > 0, lane < act - 1, PC, PC,
+                                              &ed);
     __syncwarp();  // the band is read before a_lv overwrites it
     if (lane < act) {
       T w[2 * PC];
@@ -357,15 +395,16 @@ __device__ __forceinline__ void wcompact_rev(T (&s)[PA], T* buf, const DevProgra
 }
 
 // Forward-stepping levels: band of level LV+1 has 32*P pairs.
-template <typename T, int WI, int OP, int P0, int LV>
+template <typename T, int WI, int OP, int P0, int LV, bool EDGE = false>
 __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
                                      const DevProgram<T>& prog, int levels,
-                                     int lane, int lc) {
+                                     int lane, int lc, int bc = BC_ZERO) {
   constexpr int P = P0 >> LV;
   if constexpr (P >= 1 && P >= kreach(WI, OP)) {
     if (LV < levels) {
       constexpr int NB = 32 * P;  // band length at this level
-      wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane > 0, lane < 31);
+      const WEdge<T> ed{&prog, bc, NB};
+      wsteps<T, WI, OP, 0, P, P0, false, EDGE>(s, d, prog, lane > 0, lane < 31, P, P, &ed);
       write_run<T, P, P>(buf, NB + P * lane, d);
       if (LV + 1 == levels) {
         write_run<T, P, P>(buf, P * lane, s);
@@ -374,7 +413,7 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
       if constexpr (WI == WI_GEN) {
         // the wavelet's register levels end at lc (run time)
         if (LV + 1 >= lc) {
-          wcompact_fwd<T, WI, OP, P, P0>(s, buf, prog, levels, LV + 1, lane);
+          wcompact_fwd<T, WI, OP, P, P0, EDGE>(s, buf, prog, levels, LV + 1, lane, bc);
           return;
         }
 #pragma unroll
@@ -382,26 +421,26 @@ __device__ __forceinline__ void wfwd(T (&s)[P0], T (&d)[P0], T* buf,
           d[i] = s[2 * i + 1];
           s[i] = s[2 * i];
         }
-        wfwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane, lc);
+        wfwd<T, WI, OP, P0, LV + 1, EDGE>(s, d, buf, prog, levels, lane, lc, bc);
       } else if constexpr (LV + 1 >= reg_max_levels(WI, OP, P0)) {
-        wcompact_fwd<T, WI, OP, P, P0>(s, buf, prog, levels, LV + 1, lane);
+        wcompact_fwd<T, WI, OP, P, P0, EDGE>(s, buf, prog, levels, LV + 1, lane, bc);
       } else {
 #pragma unroll
         for (int i = 0; i < P / 2; ++i) {
           d[i] = s[2 * i + 1];
           s[i] = s[2 * i];
         }
-        wfwd<T, WI, OP, P0, LV + 1>(s, d, buf, prog, levels, lane, lc);
+        wfwd<T, WI, OP, P0, LV + 1, EDGE>(s, d, buf, prog, levels, lane, lc, bc);
       }
     }
   }
 }
 
 // Reverse-stepping levels, coarsest first (LV counts down).
-template <typename T, int WI, int OP, int P0, int LV>
+template <typename T, int WI, int OP, int P0, int LV, bool EDGE = false>
 __device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
                                      const DevProgram<T>& prog, int levels,
-                                     int lane, int lc) {
+                                     int lane, int lc, int bc = BC_ZERO) {
   constexpr int P = P0 >> LV;
   if constexpr (LV >= 0) {
     if constexpr (P >= 1 && P >= kreach(WI, OP)) {
@@ -410,7 +449,8 @@ __device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
         constexpr int NB = 32 * P;
         if (LV + 1 == levels) read_run<T, P, P>(buf, P * lane, s);
         read_run<T, P, P>(buf, NB + P * lane, d);
-        wsteps<T, WI, OP, 0, P, P0>(s, d, prog, lane > 0, lane < 31);
+        const WEdge<T> ed{&prog, bc, NB};
+        wsteps<T, WI, OP, 0, P, P0, false, EDGE>(s, d, prog, lane > 0, lane < 31, P, P, &ed);
         if constexpr (LV > 0) {
 #pragma unroll
           for (int i = P - 1; i >= 0; --i) {
@@ -420,7 +460,7 @@ __device__ __forceinline__ void wrev(T (&s)[P0], T (&d)[P0], T* buf,
         }
       }
     }
-    if constexpr (LV > 0) wrev<T, WI, OP, P0, LV - 1>(s, d, buf, prog, levels, lane, lc);
+    if constexpr (LV > 0) wrev<T, WI, OP, P0, LV - 1, EDGE>(s, d, buf, prog, levels, lane, lc, bc);
   }
 }
 
@@ -457,7 +497,9 @@ constexpr int wrow_max_levels(int wi, int op, int p0) {
   return lv;
 }
 
-template <typename T, int WI, int OP, int P0>
+// EDGE: the instantiation for the Constant, Symmetric and Reflect
+// boundaries (exact band edges, lw_edge.cuh; compiled wavelets).
+template <typename T, int WI, int OP, int P0, bool EDGE = false>
 __global__ void __launch_bounds__(128)
     wrow_kernel(const __grid_constant__ WRowParams<T> p) {
   constexpr int N = 64 * P0;                  // row length
@@ -505,17 +547,18 @@ __global__ void __launch_bounds__(128)
       d[i] = x[2 * i + 1];
     }
     __syncwarp();
-    wrow::wfwd<T, WI, OP, P0, 0>(s, d, buf, p.prog, p.levels, lane, p.reg_levels);
+    wrow::wfwd<T, WI, OP, P0, 0, EDGE>(s, d, buf, p.prog, p.levels, lane, p.reg_levels, p.bc);
   } else {
     constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
     if constexpr (WI != WI_GEN) {
       if (p.levels > TOP + 1)
-        wrow::wcompact_rev<T, WI, OP, (P0 >> TOP), P0>(s, buf, p.prog, p.levels, TOP + 1, lane);
+        wrow::wcompact_rev<T, WI, OP, (P0 >> TOP), P0, EDGE>(s, buf, p.prog, p.levels, TOP + 1,
+                                                             lane, p.bc);
     } else {
       if (p.levels > p.reg_levels && p.reg_levels >= 1)
         wrow::gen_compact_rev<T, WI, OP, P0, 0>(p.reg_levels, s, buf, p.prog, p.levels, lane);
     }
-    wrow::wrev<T, WI, OP, P0, TOP>(s, d, buf, p.prog, p.levels, lane, p.reg_levels);
+    wrow::wrev<T, WI, OP, P0, TOP, EDGE>(s, d, buf, p.prog, p.levels, lane, p.reg_levels, p.bc);
     __syncwarp();
     T x[2 * P0];
 #pragma unroll

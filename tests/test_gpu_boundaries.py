@@ -4,8 +4,8 @@ of every step in the reference's order (mapped taps for Forward and
 Inverse, fold loops before and after the direct update for the adjoints,
 src/lifted-steps-inl.hpp:409-615).  Strided passes on the TMA-staged kernel
 (whole lines, windows with a chained band pass, 3D views), contiguous rows
-on the whole-line register kernel, the 2D benchmark image, and checks that
-no pass fell back to the general kernel."""
+on the warp-per-row kernel, the 2D benchmark image, and checks that no pass
+fell back to the general kernel."""
 import numpy as np
 import pytest
 
@@ -24,10 +24,11 @@ BCS = [1, 3, 4]            # Constant, Symmetric, Reflect
 def run(x, w, op, bc, axes, levels):
     t = torch.from_numpy(np.ascontiguousarray(x)).cuda()
     l0 = _lib.kernel_launches("line")
-    f0 = _lib.kernel_launches("col") + _lib.kernel_launches("reg")
+    fams = ("col", "reg", "wrow")
+    f0 = sum(_lib.kernel_launches(f) for f in fams)
     y = pl._lwt(t, w, bc, op, list(axes), list(levels), 1)
     torch.cuda.synchronize()
-    fast = _lib.kernel_launches("col") + _lib.kernel_launches("reg") - f0
+    fast = sum(_lib.kernel_launches(f) for f in fams) - f0
     return y.cpu().numpy(), _lib.kernel_launches("line") - l0, fast
 
 
@@ -68,7 +69,7 @@ def test_contiguous_rows_and_images(bc, dtype):
             lv = [max(1, min(l_, po.max_level(width, shape[a]))) for a, l_ in zip(axes, lv)]
             x = rng.standard_normal(shape).astype(dtype)
             for op in range(4):
-                check(x, w, op, bc, axes, lv, want_fast=False)
+                check(x, w, op, bc, axes, lv, want_fast=(w == 100907))
 
 
 @pytest.mark.parametrize("bc", BCS)
