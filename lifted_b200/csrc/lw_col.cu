@@ -68,8 +68,7 @@ ColFn<T> by_wavelet(int wi, int op) {
 // em: lines whose length is not a multiple of 32 (one line per lane only);
 // edge: the exact-edge instantiation (non-Zero boundaries)
 ColFn<float> pick_col_f32(int wi, int op, int v, bool em, bool edge) {
-  if (edge) return em ? nullptr : (v == 2 ? edge_wavelet<float, 2>(wi, op)
-                                          : edge_wavelet<float, 1>(wi, op));
+  if (edge) return (em || v != 1) ? nullptr : edge_wavelet<float, 1>(wi, op);
   if (em) return v == 1 ? by_wavelet<float, 1, true>(wi, op) : nullptr;
   return v == 2 ? by_wavelet<float, 2, false>(wi, op) : by_wavelet<float, 1, false>(wi, op);
 }

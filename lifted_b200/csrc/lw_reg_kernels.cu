@@ -314,9 +314,13 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   // instantiation, compiled wavelets only
   const bool zero = a.bc == BC_ZERO;
   if (!zero && gen) return 0;
+  const int F = edge_footprint(*a.prog, a.bc);
+  if (F < 0) return 0;
   if constexpr (sizeof(T) == 4) {
     const int64_t q0 = g.n / 128;
-    if (zero && !gen && wrow2_enabled() && g.n % 128 == 0 && (q0 == 16 || q0 == 32) &&
+    // non-Zero boundaries: every level's lanes hold the edge reach
+    const bool edge_fits = zero || (a.levels >= 1 && (q0 >> (a.levels - 1)) >= F);
+    if (!gen && edge_fits && wrow2_enabled() && g.n % 128 == 0 && (q0 == 16 || q0 == 32) &&
         wrow2_levels_f32(a.wi, a.op, (int)q0) >= a.levels) {
       WRowParams<T> p;
       std::memset(&p, 0, sizeof(p));
@@ -325,12 +329,13 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       p.g = g;
       p.levels = a.levels;
       p.l2hint = l2_hint_code();
+      p.bc = a.bc;
       p.prog = *a.prog;
       const size_t smem = (size_t)4 * (size_t)g.n * sizeof(T);
       const int64_t grid = std::min<int64_t>((g.nlines + 1) / 2,
                                              (int64_t)sm_count() * wrow2_resident_ctas((int)q0));
       if (grid <= 0x7fffffffLL) {
-        cudaError_t e = launch_wrow2_f32(a.wi, a.op, (int)q0, p, (int)grid, smem, stream);
+        cudaError_t e = launch_wrow2_f32(a.wi, a.op, (int)q0, p, (int)grid, smem, stream, !zero);
         if (e != cudaSuccess) return -(int)e - 1000;
         counted(stats, KF_WROW2);
         return 1;
@@ -356,8 +361,6 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   if (!zero) {
     // every level's lanes must hold the edge work's reach: the register
     // levels' pairs, then the compacted lanes' pairs
-    const int F = edge_footprint(*a.prog, a.bc);
-    if (F < 0) return 0;
     const int lreg = reg_max_levels(a.wi, a.op, (int)p0);
     for (int j = 0; j < std::min(lreg, a.levels); ++j)
       if (((int)p0 >> j) < F) return 0;
@@ -754,6 +757,9 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     const int wk = wide ? WI_GENW : (gen ? WI_GEN : wi);
     ColFn<T> fn;
     if (em) v = 1;
+    // the exact-edge instantiation packs one line per lane (with two, its
+    // edge work overflows the registers)
+    if (a.bc != BC_ZERO) v = 1;
     if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v, em, a.bc != BC_ZERO);
     else fn = pick_col_f64(wk, op, em, a.bc != BC_ZERO);
     if (!fn) return 0;

@@ -26,7 +26,7 @@ cudaError_t launch_wrow_f64(int wi, int op, int p0, const WRowParams<double>& p,
 // threads = two rows per CTA): levels compiled, 0 if none; launcher.
 int wrow2_levels_f32(int wi, int op, int p0);
 cudaError_t launch_wrow2_f32(int wi, int op, int p0, const WRowParams<float>& p, int grid,
-                             size_t smem, cudaStream_t stream);
+                             size_t smem, cudaStream_t stream, bool edge);
 // CTAs per SM the two-warp kernel's shared memory allows (grid sizing of
 // the persistent launch).
 int wrow2_resident_ctas(int p0);

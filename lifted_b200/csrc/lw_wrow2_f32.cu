@@ -10,9 +10,9 @@ namespace lw {
 
 namespace {
 
-template <int WI, int OP, int P0>
+template <int WI, int OP, int P0, bool EDGE>
 cudaError_t launch_one(const WRowParams<float>& p, int grid, size_t smem, cudaStream_t stream) {
-  auto kern = wrow2_kernel<WI, OP, P0>;
+  auto kern = wrow2_kernel<WI, OP, P0, EDGE>;
   static bool configured[kMaxDevices] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -29,22 +29,22 @@ cudaError_t launch_one(const WRowParams<float>& p, int grid, size_t smem, cudaSt
 
 using Fn = cudaError_t (*)(const WRowParams<float>&, int, size_t, cudaStream_t);
 
-template <int WI, int P0>
+template <int WI, int P0, bool EDGE>
 Fn by_op(int op) {
   switch (op) {
-    case 0: return launch_one<WI, 0, P0>;
-    case 1: return launch_one<WI, 1, P0>;
-    case 2: return launch_one<WI, 2, P0>;
-    default: return launch_one<WI, 3, P0>;
+    case 0: return launch_one<WI, 0, P0, EDGE>;
+    case 1: return launch_one<WI, 1, P0, EDGE>;
+    case 2: return launch_one<WI, 2, P0, EDGE>;
+    default: return launch_one<WI, 3, P0, EDGE>;
   }
 }
 
-template <int P0>
+template <int P0, bool EDGE>
 Fn by_wavelet(int wi, int op) {
   switch (wi) {
-    case 2: return by_op<2, P0>(op);
-    case 4: return by_op<4, P0>(op);
-    case 33: return by_op<33, P0>(op);
+    case 2: return by_op<2, P0, EDGE>(op);
+    case 4: return by_op<4, P0, EDGE>(op);
+    case 33: return by_op<33, P0, EDGE>(op);
     default: return nullptr;
   }
 }
@@ -58,8 +58,10 @@ int wrow2_levels_f32(int wi, int op, int p0) {
 }
 
 cudaError_t launch_wrow2_f32(int wi, int op, int p0, const WRowParams<float>& p, int grid,
-                             size_t smem, cudaStream_t stream) {
-  Fn fn = p0 == 16 ? by_wavelet<16>(wi, op) : (p0 == 32 ? by_wavelet<32>(wi, op) : nullptr);
+                             size_t smem, cudaStream_t stream, bool edge) {
+  Fn fn = nullptr;
+  if (p0 == 16) fn = edge ? by_wavelet<16, true>(wi, op) : by_wavelet<16, false>(wi, op);
+  if (p0 == 32) fn = edge ? by_wavelet<32, true>(wi, op) : by_wavelet<32, false>(wi, op);
   if (!fn) return cudaErrorInvalidValue;
   return fn(p, grid, smem, stream);
 }

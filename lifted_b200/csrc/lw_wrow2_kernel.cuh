@@ -48,9 +48,13 @@ __device__ __forceinline__ void row_sync(int id) {
 
 // One step over the lane's P pairs: halos by shuffle inside each warp, and
 // across the seam of the row's two warps through the mailbox.
-template <int P, int PA, int HMAX, int KIND, int OFF, int NT, int SUB, int HL, int HR>
+// EDGE: the lanes holding the row band's ends (global lanes 0 and 63) redo
+// their edge around the Zero update for the Constant, Symmetric and Reflect
+// boundaries (lw_edge.cuh).
+template <int P, int PA, int HMAX, int KIND, int OFF, int NT, int SUB, int HL, int HR,
+          bool EDGE = false>
 __device__ __forceinline__ void update(float (&y)[PA], const float (&x)[PA], const DevStep<float>& st,
-                                       Seam& sm) {
+                                       Seam& sm, const wrow::WEdge<float>* ed = nullptr) {
   static_assert(HL <= P && HR <= P, "step reaches past the neighbour lane");
   float xl[HL > 0 ? HL : 1], xr[HR > 0 ? HR : 1];
 #pragma unroll
@@ -82,6 +86,17 @@ __device__ __forceinline__ void update(float (&y)[PA], const float (&x)[PA], con
   }
   const int g = sm.half * 32 + sm.lane;
   const bool okl = g > 0, okr = g < GL - 1;
+  constexpr int E = P < edge::kEdge ? P : edge::kEdge;
+  float sf[HL > 0 ? HL : 1], sb[HR > 0 ? HR : 1];
+  bool efront = false, eback = false;
+  if constexpr (EDGE) {
+    efront = ed->bc != BC_ZERO && !okl;
+    eback = ed->bc != BC_ZERO && !okr;
+    if (efront)
+      edge::call<P, E, false>(st, *ed->prog, ed->bc, false, y, x, sf, 0, ed->nb, HL, HR);
+    if (eback)
+      edge::call<P, E, true>(st, *ed->prog, ed->bc, false, y, x, sb, ed->nb - P, ed->nb, HL, HR);
+  }
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     float yi = y[i];
@@ -116,11 +131,17 @@ __device__ __forceinline__ void update(float (&y)[PA], const float (&x)[PA], con
     }
     y[i] = yi;
   }
+  if constexpr (EDGE) {
+    if (efront)
+      edge::call<P, E, false>(st, *ed->prog, ed->bc, true, y, x, sf, 0, ed->nb, HL, HR);
+    if (eback)
+      edge::call<P, E, true>(st, *ed->prog, ed->bc, true, y, x, sb, ed->nb - P, ed->nb, HL, HR);
+  }
 }
 
-template <int WI, int OP, int K, int P, int PA, int HMAX>
+template <int WI, int OP, int K, int P, int PA, int HMAX, bool EDGE = false>
 __device__ __forceinline__ void steps(float (&s)[PA], float (&d)[PA], const DevProgram<float>& prog,
-                                      Seam& sm) {
+                                      Seam& sm, const wrow::WEdge<float>* ed = nullptr) {
   if constexpr (K < cat_nsteps(WI)) {
     constexpr CStep cs = cstep(WI, OP, K);
     const DevStep<float>& st = prog.st[K];
@@ -132,23 +153,27 @@ __device__ __forceinline__ void steps(float (&s)[PA], float (&d)[PA], const DevP
         d[i] = d[i] * dmul;
       }
     } else if constexpr (cs.y_is_d) {
-      update<P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(d, s, st, sm);
+      update<P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EDGE>(d, s, st, sm,
+                                                                                    ed);
     } else {
-      update<P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right>(s, d, st, sm);
+      update<P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EDGE>(s, d, st, sm,
+                                                                                    ed);
     }
-    steps<WI, OP, K + 1, P, PA, HMAX>(s, d, prog, sm);
+    steps<WI, OP, K + 1, P, PA, HMAX, EDGE>(s, d, prog, sm, ed);
   }
 }
 
-template <int WI, int OP, int P0, int HMAX, int LV>
+template <int WI, int OP, int P0, int HMAX, int LV, bool EDGE = false>
 __device__ __forceinline__ void fwd(float (&s)[P0], float (&d)[P0], float* buf,
-                                    const DevProgram<float>& prog, int levels, Seam& sm) {
+                                    const DevProgram<float>& prog, int levels, Seam& sm,
+                                    int bc = BC_ZERO) {
   constexpr int P = P0 >> LV;
   if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
     if (LV < levels) {
       constexpr int NB = GL * P;
       const int g = sm.half * 32 + sm.lane;
-      steps<WI, OP, 0, P, P0, HMAX>(s, d, prog, sm);
+      const wrow::WEdge<float> ed{&prog, bc, NB};
+      steps<WI, OP, 0, P, P0, HMAX, EDGE>(s, d, prog, sm, &ed);
       wrow::write_run<float, P, P>(buf, NB + P * g, d);
       if (LV + 1 == levels) {
         wrow::write_run<float, P, P>(buf, P * g, s);
@@ -159,14 +184,15 @@ __device__ __forceinline__ void fwd(float (&s)[P0], float (&d)[P0], float* buf,
         d[i] = s[2 * i + 1];
         s[i] = s[2 * i];
       }
-      fwd<WI, OP, P0, HMAX, LV + 1>(s, d, buf, prog, levels, sm);
+      fwd<WI, OP, P0, HMAX, LV + 1, EDGE>(s, d, buf, prog, levels, sm, bc);
     }
   }
 }
 
-template <int WI, int OP, int P0, int HMAX, int LV>
+template <int WI, int OP, int P0, int HMAX, int LV, bool EDGE = false>
 __device__ __forceinline__ void rev(float (&s)[P0], float (&d)[P0], float* buf,
-                                    const DevProgram<float>& prog, int levels, Seam& sm) {
+                                    const DevProgram<float>& prog, int levels, Seam& sm,
+                                    int bc = BC_ZERO) {
   constexpr int P = P0 >> LV;
   if constexpr (LV >= 0) {
     if constexpr (P >= 1 && P >= cat_reach(WI, OP)) {
@@ -175,7 +201,8 @@ __device__ __forceinline__ void rev(float (&s)[P0], float (&d)[P0], float* buf,
         const int g = sm.half * 32 + sm.lane;
         if (LV + 1 == levels) wrow::read_run<float, P, P>(buf, P * g, s);
         wrow::read_run<float, P, P>(buf, NB + P * g, d);
-        steps<WI, OP, 0, P, P0, HMAX>(s, d, prog, sm);
+        const wrow::WEdge<float> ed{&prog, bc, NB};
+        steps<WI, OP, 0, P, P0, HMAX, EDGE>(s, d, prog, sm, &ed);
         if constexpr (LV > 0) {
 #pragma unroll
           for (int i = P - 1; i >= 0; --i) {
@@ -185,7 +212,7 @@ __device__ __forceinline__ void rev(float (&s)[P0], float (&d)[P0], float* buf,
         }
       }
     }
-    if constexpr (LV > 0) rev<WI, OP, P0, HMAX, LV - 1>(s, d, buf, prog, levels, sm);
+    if constexpr (LV > 0) rev<WI, OP, P0, HMAX, LV - 1, EDGE>(s, d, buf, prog, levels, sm, bc);
   }
 }
 
@@ -195,7 +222,9 @@ __device__ __forceinline__ void rev(float (&s)[P0], float (&d)[P0], float* buf,
 // Persistent: each slot walks rows blockIdx.x*2 + slot, + 2*gridDim.x, ...
 // with two row buffers, the next row's cp.async copy in flight while the
 // current row is lifted and stored.
-template <int WI, int OP, int P0>
+// EDGE: the instantiation for the Constant, Symmetric and Reflect
+// boundaries (exact band edges; every level's lanes hold the edge reach).
+template <int WI, int OP, int P0, bool EDGE = false>
 __global__ void __launch_bounds__(128)
     wrow2_kernel(const __grid_constant__ WRowParams<float> p) {
   constexpr int N = 128 * P0;     // row length
@@ -254,10 +283,10 @@ __global__ void __launch_bounds__(128)
         d[i] = x[2 * i + 1];
       }
       wrow2::row_sync(sm.bar_id);
-      wrow2::fwd<WI, OP, P0, HMAX, 0>(s, d, buf, p.prog, p.levels, sm);
+      wrow2::fwd<WI, OP, P0, HMAX, 0, EDGE>(s, d, buf, p.prog, p.levels, sm, p.bc);
     } else {
       constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
-      wrow2::rev<WI, OP, P0, HMAX, TOP>(s, d, buf, p.prog, p.levels, sm);
+      wrow2::rev<WI, OP, P0, HMAX, TOP, EDGE>(s, d, buf, p.prog, p.levels, sm, p.bc);
       wrow2::row_sync(sm.bar_id);
       float x[2 * P0];
 #pragma unroll
