@@ -86,6 +86,7 @@ std::atomic<int64_t> g_opt_generic{1};
 std::atomic<int64_t> g_opt_l2_hints{0};
 std::atomic<int64_t> g_opt_col_row_order{1};
 std::atomic<int64_t> g_opt_batch_nd_mode{0};
+std::atomic<int64_t> g_opt_edge_always{0};
 
 }  // namespace
 
@@ -864,6 +865,8 @@ int set_option(const char* name, int64_t value) {
     g_opt_l2_hints = value ? 1 : 0;
   } else if (!std::strcmp(name, "col_row_order")) {
     g_opt_col_row_order = value ? 1 : 0;
+  } else if (!std::strcmp(name, "edge_kernels_always")) {
+    g_opt_edge_always = value ? 1 : 0;
   } else if (!std::strcmp(name, "batch_nd_mode")) {
     if (value < 0 || value > 2) return set_error(LIFTED_EINVAL, "batch_nd_mode outside 0..2");
     g_opt_batch_nd_mode = value;
@@ -882,6 +885,7 @@ bool col_packed() { return g_opt_tma_packed.load() != 0; }
 bool col_stacked() { return g_opt_tma_stacked.load() != 0; }
 bool col_row_order() { return g_opt_col_row_order.load() != 0; }
 int batch_nd_mode() { return (int)g_opt_batch_nd_mode.load(); }
+bool edge_kernels_always() { return g_opt_edge_always.load() != 0; }
 bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
 bool pdl_enabled() { return g_opt_overlap.load() != 0; }
 bool wtile_enabled() { return g_opt_row_windows.load() != 0; }

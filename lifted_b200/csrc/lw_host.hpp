@@ -89,6 +89,10 @@ int run_batch_nd(uint32_t op, uint32_t bc, size_t nimg, const lifted_image_t* im
                  T* out, cudaStream_t stream, bool* ran);
 // The "batch_nd_mode" option: 0 automatic, 1 persistent, 2 grouped.
 int batch_nd_mode();
+// The "edge_kernels_always" option: Zero passes run the exact-edge kernel
+// instantiations too (their edge work then never runs; for comparing the
+// two instantiations).
+bool edge_kernels_always();
 // Per-axis levels of the separable driver, resolved and checked (level 0 =
 // max_level; degenerate bands refused), as lifted_lwt_sep_* does.
 int resolve_sep_levels(const Program& prog, uint32_t op, uint32_t bc,

@@ -293,7 +293,7 @@ int launch_whole(const RegPassArgs<T>& a, const LineGeom& g, const T* in,
   p.prog = *a.prog;
   const int64_t groups = (g.nlines + lines_cta - 1) / lines_cta;
   if (groups > 0x7fffffffLL) return 0;
-  RegFn<T> fn = pick<T>(wi, op, strided, false, v, a.bc != BC_ZERO);
+  RegFn<T> fn = pick<T>(wi, op, strided, false, v, a.bc != BC_ZERO || edge_kernels_always());
   if (!fn) return 0;
   cudaError_t e = fn(p, (int)groups, block, smem, stream);
   if (e != cudaSuccess) return -(int)e - 1000;
@@ -335,7 +335,8 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
       const int64_t grid = std::min<int64_t>((g.nlines + 1) / 2,
                                              (int64_t)sm_count() * wrow2_resident_ctas((int)q0));
       if (grid <= 0x7fffffffLL) {
-        cudaError_t e = launch_wrow2_f32(a.wi, a.op, (int)q0, p, (int)grid, smem, stream, !zero);
+        cudaError_t e = launch_wrow2_f32(a.wi, a.op, (int)q0, p, (int)grid, smem, stream,
+                                         !zero || edge_kernels_always());
         if (e != cudaSuccess) return -(int)e - 1000;
         counted(stats, KF_WROW2);
         return 1;
@@ -389,9 +390,11 @@ int launch_wrow(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
   if (grid > 0x7fffffffLL) return 0;
   cudaError_t e;
   if constexpr (sizeof(T) == 4)
-    e = launch_wrow_f32(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream, !zero);
+    e = launch_wrow_f32(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream,
+                        (!zero || edge_kernels_always()) && !gen);
   else
-    e = launch_wrow_f64(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream, !zero);
+    e = launch_wrow_f64(wk, a.op, (int)p0, p, (int)grid, 32 * warps, smem, stream,
+                        (!zero || edge_kernels_always()) && !gen);
   if (e != cudaSuccess) return -(int)e - 1000;
   counted(stats, KF_WROW);
   return 1;
@@ -517,7 +520,7 @@ int launch_tiled(const RegPassArgs<T>& a, cudaStream_t stream,
   p.halo = halo;
   p.ntiles = ntiles;
   p.prog = *a.prog;
-  RegFn<T> tfn = pick<T>(wi, op, true, true, v, a.bc != BC_ZERO);
+  RegFn<T> tfn = pick<T>(wi, op, true, true, v, a.bc != BC_ZERO || edge_kernels_always());
   if (!tfn) {
     if (tmp) scratch_free(tmp, stream);
     return 0;
@@ -759,9 +762,10 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (em) v = 1;
     // the exact-edge instantiation packs one line per lane (with two, its
     // edge work overflows the registers)
-    if (a.bc != BC_ZERO) v = 1;
-    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v, em, a.bc != BC_ZERO);
-    else fn = pick_col_f64(wk, op, em, a.bc != BC_ZERO);
+    const bool edge_inst = (a.bc != BC_ZERO || edge_kernels_always()) && compiled_wavelet(wi) && !em;
+    if (edge_inst) v = 1;
+    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v, em, edge_inst);
+    else fn = pick_col_f64(wk, op, em, edge_inst);
     if (!fn) return 0;
     const int64_t m = n >> k;
     const bool more = a.levels > k;

@@ -24,7 +24,7 @@ BCS = [1, 3, 4]            # Constant, Symmetric, Reflect
 def run(x, w, op, bc, axes, levels):
     t = torch.from_numpy(np.ascontiguousarray(x)).cuda()
     l0 = _lib.kernel_launches("line")
-    fams = ("col", "reg", "wrow")
+    fams = ("col", "reg", "wrow", "wrow2")
     f0 = sum(_lib.kernel_launches(f) for f in fams)
     y = pl._lwt(t, w, bc, op, list(axes), list(levels), 1)
     torch.cuda.synchronize()
