@@ -24,7 +24,7 @@ cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
-  return launch_overlapped(kern, grid, COL_THREADS, smem, stream, p);
+  return launch_overlapped_kind(1, kern, grid, COL_THREADS, smem, stream, p);
 }
 
 template <typename T, int WI, int V, bool EM, bool EDGE = false>

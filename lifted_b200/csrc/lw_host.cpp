@@ -87,6 +87,7 @@ std::atomic<int64_t> g_opt_l2_hints{0};
 std::atomic<int64_t> g_opt_col_row_order{1};
 std::atomic<int64_t> g_opt_batch_nd_mode{0};
 std::atomic<int64_t> g_opt_edge_always{0};
+std::atomic<int64_t> g_opt_overlap_graphs{0};
 
 }  // namespace
 
@@ -865,6 +866,9 @@ int set_option(const char* name, int64_t value) {
     g_opt_l2_hints = value ? 1 : 0;
   } else if (!std::strcmp(name, "col_row_order")) {
     g_opt_col_row_order = value ? 1 : 0;
+  } else if (!std::strcmp(name, "overlap_in_graphs")) {
+    if (value < 0 || value > 2) return set_error(LIFTED_EINVAL, "overlap_in_graphs outside 0..2");
+    g_opt_overlap_graphs = value;
   } else if (!std::strcmp(name, "edge_kernels_always")) {
     g_opt_edge_always = value ? 1 : 0;
   } else if (!std::strcmp(name, "batch_nd_mode")) {
@@ -888,6 +892,10 @@ int batch_nd_mode() { return (int)g_opt_batch_nd_mode.load(); }
 bool edge_kernels_always() { return g_opt_edge_always.load() != 0; }
 bool wrow2_enabled() { return g_opt_wrow_split.load() != 0; }
 bool pdl_enabled() { return g_opt_overlap.load() != 0; }
+bool pdl_in_graphs(int kind) {
+  const int64_t v = g_opt_overlap_graphs.load();
+  return v == 1 || (v == 2 && kind == 1);
+}
 bool wtile_enabled() { return g_opt_row_windows.load() != 0; }
 bool generic_enabled() { return g_opt_generic.load() != 0; }
 int l2_hint_code() {

@@ -22,10 +22,14 @@ namespace lw {
 
 // Whether launches use the attribute (the "overlap_launches" option).
 bool pdl_enabled();
+// Whether launches recorded by stream capture use it too (the
+// "overlap_in_graphs" option: 0 none, 1 every launch, 2 the TMA-staged
+// strided kernel's launches only); kind 1 marks those launches.
+bool pdl_in_graphs(int kind);
 
 template <typename... KArgs, typename... Args>
-cudaError_t launch_overlapped(void (*kern)(KArgs...), int grid, int block, size_t smem,
-                              cudaStream_t stream, Args&&... args) {
+cudaError_t launch_overlapped_kind(int kind, void (*kern)(KArgs...), int grid, int block,
+                                   size_t smem, cudaStream_t stream, Args&&... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3((unsigned)block);
@@ -40,8 +44,15 @@ cudaError_t launch_overlapped(void (*kern)(KArgs...), int grid, int block, size_
     cudaGetLastError();  // clear it: the launch below reports its own
     cap = cudaStreamCaptureStatusActive;
   }
-  cfg.numAttrs = (pdl_enabled() && cap == cudaStreamCaptureStatusNone) ? 1 : 0;
+  cfg.numAttrs =
+      (pdl_enabled() && (cap == cudaStreamCaptureStatusNone || pdl_in_graphs(kind))) ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_overlapped(void (*kern)(KArgs...), int grid, int block, size_t smem,
+                              cudaStream_t stream, Args&&... args) {
+  return launch_overlapped_kind(0, kern, grid, block, smem, stream, std::forward<Args>(args)...);
 }
 
 #ifdef __CUDACC__
