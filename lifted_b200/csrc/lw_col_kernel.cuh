@@ -248,7 +248,7 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
           if (c.tid == 0 && rs.next < rs.p->ntiles)
             issue<T, false, V>(*rs.p, rs.next, const_cast<T*>(rs.stage), rs.bar);
         }
-        reg::steps<T, VT, WI, OP, 0, P, P0, HMAX, EM, EDGE>(s, d, c, gp0, nb);
+        reg::steps_sel<T, VT, WI, OP, P, P0, HMAX, EM, EDGE>(s, d, c, gp0, nb);
         if constexpr (LV == 0) {
           if (reg::chunk_stored(c)) {
             T* o = p.out + c.bout + c.e0 * p.g.sout;

@@ -380,6 +380,25 @@ __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
   }
 }
 
+// The steps of one level in an exact-edge instantiation: a warp with a
+// lane on a band end runs the edge-aware step code, every other warp the
+// Zero step code, which has no call to the edge routine and compiles like
+// the Zero kernels' (the call otherwise constrains the code around it).
+// The choice is warp-uniform, and both forms take the same barriers.
+template <typename T, typename VT, int WI, int OP, int P, int PA, int HMAX, bool EM, bool EDGE>
+__device__ __forceinline__ void steps_sel(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c, int64_t gp0,
+                                          int64_t nb) {
+  if constexpr (EDGE) {
+    const bool mine = c.bc != BC_ZERO && c.line_ok && (gp0 == 0 || gp0 + P == nb);
+    if (__any_sync(0xffffffffu, mine))
+      steps<T, VT, WI, OP, 0, P, PA, HMAX, EM, true>(s, d, c, gp0, nb);
+    else
+      steps<T, VT, WI, OP, 0, P, PA, HMAX, EM, false>(s, d, c, gp0, nb);
+  } else {
+    steps<T, VT, WI, OP, 0, P, PA, HMAX, EM, false>(s, d, c, gp0, nb);
+  }
+}
+
 // Stores P consecutive band values v[0..P) at line positions pos0.. of the
 // destination (vectorised for unit-stride aligned rows; with V lines per
 // lane, one V-wide store per position covers the lane's adjacent lines).
@@ -441,7 +460,7 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
         const int64_t rem = nb - gp0;
         lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
       }
-      steps<T, VT, WI, OP, 0, P, P0, HMAX, EM, EDGE>(s, d, c, gp0, nb);
+      steps_sel<T, VT, WI, OP, P, P0, HMAX, EM, EDGE>(s, d, c, gp0, nb);
       if (chunk_stored(c)) {
         if constexpr (EM) store_first<T, VT, P, P0>(d, c, nb + gp0, lim);
         else store_run<T, VT, P, P0>(d, c, nb + gp0);
@@ -535,7 +554,7 @@ __device__ __forceinline__ void rev_levels(VT (&s)[P0], VT (&d)[P0],
                      ? *reinterpret_cast<const VT*>(p.in + c.bin + (nb + q) * p.g.sin)
                      : vzero<VT>();
         }
-        steps<T, VT, WI, OP, 0, P, P0, HMAX, false, EDGE>(s, d, c, gp0, nb);
+        steps_sel<T, VT, WI, OP, P, P0, HMAX, false, EDGE>(s, d, c, gp0, nb);
         if constexpr (LV == 0) {
           if (chunk_stored(c)) {
             T* o = p.out + c.bout + c.e0 * p.g.sout;
