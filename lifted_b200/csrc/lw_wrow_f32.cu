@@ -8,6 +8,10 @@
 
 namespace lw {
 
+// The exact-edge instantiations (lw_wrow_f32_edge.cu).
+using WRowFnf32 = cudaError_t (*)(const WRowParams<float>&, int, int, size_t, cudaStream_t);
+WRowFnf32 wrow_edge_f32(int wi, int op, int p0);
+
 namespace {
 
 template <int WI, int OP, int P0, bool EDGE>
@@ -51,17 +55,6 @@ Fn by_wavelet(int wi, int op) {
   }
 }
 
-// The exact-edge instantiations (Constant, Symmetric, Reflect) of the
-// compiled wavelets.
-template <int P0>
-Fn edge_wavelet(int wi, int op) {
-  switch (wi) {
-    case 2: return by_op<2, P0, true>(op);
-    case 4: return by_op<4, P0, true>(op);
-    case 33: return by_op<33, P0, true>(op);
-    default: return nullptr;
-  }
-}
 
 }  // namespace
 
@@ -80,10 +73,10 @@ cudaError_t launch_wrow_f32(int wi, int op, int p0, const WRowParams<float>& p,
                             cudaStream_t stream, bool edge) {
   Fn fn = nullptr;
   switch (p0) {
-    case 8: fn = edge ? edge_wavelet<8>(wi, op) : by_wavelet<8>(wi, op); break;
-    case 16: fn = edge ? edge_wavelet<16>(wi, op) : by_wavelet<16>(wi, op); break;
-    case 32: fn = edge ? edge_wavelet<32>(wi, op) : by_wavelet<32>(wi, op); break;
-    case 64: fn = edge ? edge_wavelet<64>(wi, op) : by_wavelet<64>(wi, op); break;
+    case 8: fn = edge ? wrow_edge_f32(wi, op, 8) : by_wavelet<8>(wi, op); break;
+    case 16: fn = edge ? wrow_edge_f32(wi, op, 16) : by_wavelet<16>(wi, op); break;
+    case 32: fn = edge ? wrow_edge_f32(wi, op, 32) : by_wavelet<32>(wi, op); break;
+    case 64: fn = edge ? wrow_edge_f32(wi, op, 64) : by_wavelet<64>(wi, op); break;
     default: break;
   }
   if (!fn) return cudaErrorInvalidValue;
