@@ -24,9 +24,9 @@ ColFn<double> pick_col_f64(int wi, int op, bool em, bool edge) {
   return pick_col_f64_zero(wi, op, em);
 }
 
-size_t col_smem_bytes(int hmax, int v, int elem_bytes) {
+size_t col_smem_bytes(int hmax, int v, int elem_bytes, int mb_bufs) {
   return (size_t)COL_ROWS * COL_LANES * v * elem_bytes +
-         (size_t)4 * hmax * COL_THREADS * v * elem_bytes + 16;
+         (size_t)2 * mb_bufs * hmax * COL_THREADS * v * elem_bytes + 16;
 }
 
 }  // namespace lw

@@ -19,7 +19,8 @@ using ColFn = cudaError_t (*)(const ColParams<T>&, int, size_t, cudaStream_t);
 // and Reflect boundaries (compiled wavelets, whole chunks).
 ColFn<float> pick_col_f32(int wi, int op, int v, bool em, bool edge);
 ColFn<double> pick_col_f64(int wi, int op, bool em, bool edge);
-// Dynamic shared memory of one CTA: staging buffer, mailbox, mbarrier.
-size_t col_smem_bytes(int hmax, int v, int elem_bytes);
+// Dynamic shared memory of one CTA: staging buffer, mailbox (mb_bufs
+// buffers), mbarrier.
+size_t col_smem_bytes(int hmax, int v, int elem_bytes, int mb_bufs);
 
 }  // namespace lw

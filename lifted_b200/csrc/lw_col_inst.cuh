@@ -61,7 +61,7 @@ ColFn<T> by_wavelet(int wi, int op) {
     case 33: return by_op<T, 33, V, EM>(op);
     case WI_GEN: return by_op<T, WI_GEN, V, EM>(op);
     case WI_GENW:
-      if constexpr (sizeof(T) == 4 && V == 1) return by_op<T, WI_GENW, V, EM>(op);
+      if constexpr (V == 1) return by_op<T, WI_GENW, V, EM>(op);
       else return nullptr;
     default: return nullptr;
   }

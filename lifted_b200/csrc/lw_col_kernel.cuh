@@ -47,6 +47,15 @@ constexpr int COL_ROWS = 2 * COL_P0 * COL_CHUNKS;      // 512 window samples
 constexpr int COL_THREADS = COL_LANES * COL_CHUNKS;    // 512
 constexpr int COL_MAXK = 5;                            // levels per tile launch
 
+// Mailbox buffers of an instantiation: float64 with the wide generic
+// exchange keeps one (its staging buffer and a double-buffered mailbox do
+// not fit shared memory together), at the price of a second barrier per
+// step; every other instantiation alternates two.
+template <typename T, int WI>
+constexpr int col_mb_bufs() {
+  return (sizeof(T) == 8 && WI == WI_GENW) ? 1 : 2;
+}
+
 template <typename T>
 struct ColParams {
   // tm_rows[i]: the input viewed as {lines (x), axis (y)[, outer (z)]},
@@ -297,7 +306,8 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   extern __shared__ __align__(128) unsigned char col_smem[];
   T* stage = reinterpret_cast<T*>(col_smem);
   T* mbox = stage + COL_ROWS * W;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(mbox + 4 * HMAX * COL_THREADS * V);
+  constexpr int MBB = col_mb_bufs<T, WI>();
+  uint64_t* bar = reinterpret_cast<uint64_t*>(mbox + 2 * MBB * HMAX * COL_THREADS * V);
 
   const int tid = threadIdx.x;
   reg::Ctx<T> c;
@@ -307,6 +317,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   c.mb = mbox;
   c.cA = nullptr;
   c.cB = nullptr;
+  c.mb_bufs = MBB;
   c.j = tid % COL_LANES;
   c.r = tid / COL_LANES;
   c.tid_l = tid - COL_LANES;

@@ -211,6 +211,8 @@ struct Ctx {
   bool has_l, has_r, line_ok;
   int64_t L, bin, bout, n, e0, tile_lo, tile_hi;
   int buf;
+  int mb_bufs;      // mailbox buffers: 2 (alternating, one barrier per
+                    // step) or 1 (a second barrier after the reads)
   int bc;           // boundary condition of the pass
   uint64_t pol_st;  // L2 policy of the band stores
 };
@@ -262,7 +264,7 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
 #pragma unroll
   for (int h = 0; h < HL; ++h) mb_last[h * nth + c.tid] = x[P - HL + h];
   __syncthreads();
-  c.buf ^= 1;
+  if (c.mb_bufs == 2) c.buf ^= 1;
   if constexpr (EDGE) {
     if (efront) edge::call<P, E, false>(st, prog, c.bc, false, y, x, sf, gp0, nb, HL, HR);
     if (eback) edge::call<P, E, true>(st, prog, c.bc, false, y, x, sb, gp0, nb, HL, HR);
@@ -279,6 +281,7 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
     xr[h] = c.has_r ? mb_first[h * nth + c.tid_r] : vzero<VT>();
     vr[h] = (gp0 + P + h) < nb;
   }
+  if (c.mb_bufs == 1) __syncthreads();  // the mailbox is read before the next step writes it
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     VT yi = y[i];
@@ -646,6 +649,7 @@ __global__ void __launch_bounds__(512)
   c.has_l = c.r > 0;
   c.has_r = c.r < p.tpl - 1;
   c.buf = 0;
+  c.mb_bufs = 2;
   c.bc = p.bc;
   c.pol_st = l2_store_policy(p.l2hint);
   int64_t tile_idx = 0, group = blockIdx.x;

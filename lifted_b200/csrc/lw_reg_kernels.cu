@@ -755,7 +755,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // reach above the generic exchange width: the wide instantiation
     // (float32, one line per lane)
     const bool wide = gen && cat_reach(wi, op) > kGenHmax;
-    if (wide && (EB != 4 || cat_reach(wi, op) > kGenWideHmax)) return 0;
+    if (wide && cat_reach(wi, op) > kGenWideHmax) return 0;
     if (wide) v = 1;
     const int wk = wide ? WI_GENW : (gen ? WI_GEN : wi);
     ColFn<T> fn;
@@ -855,7 +855,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     const int hmax = wide ? kGenWideHmax
                      : gen ? kGenHmax
                            : (cat_reach(wi, op) > 0 ? cat_reach(wi, op) : 1);
-    const size_t smem = col_smem_bytes(hmax, v, EB);
+    const size_t smem = col_smem_bytes(hmax, v, EB, (EB == 8 && wide) ? 1 : 2);
     if (smem > kMaxDynSmem) {
       if (tmp) scratch_free(tmp, stream);
       return 0;

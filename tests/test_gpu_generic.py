@@ -160,3 +160,30 @@ def test_columns_of_partial_line_groups(op, dtype):
             g, _ = run(x, w, op, axes, lv)
             assert np.array_equal(g, o), (w, shape, axes, lv)
     assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
+
+
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_float64_strided_passes_take_the_same_kernels_as_float32(op):
+    """Every catalogue wavelet's strided pass, the wide-reach ones (reach
+    6-9, single-buffered mailbox in float64) included: float64 falls back to
+    the general line kernel exactly where float32 does, and both are bit for
+    bit equal to the oracle."""
+    rng = np.random.default_rng(180 + op)
+    shape = (2048, 64)
+    for w in po.wavelet_values():
+        width = po.wavelet_width(w)
+        mx = po.max_level(width, shape[0]) if width > 1 else int(np.log2(shape[0]))
+        lv = max(1, min(4, mx))
+        general = {}
+        for dtype in (np.float32, np.float64):
+            x = rng.standard_normal(shape).astype(dtype)
+            rc, o = po.oracle_sep(x, w, op, 0, [0], [lv])
+            if rc:
+                break
+            l0 = _lib.kernel_launches("line")
+            g, _ = run(x, w, op, [0], [lv])
+            general[dtype] = _lib.kernel_launches("line") - l0
+            assert np.array_equal(g, o), (w, dtype, lv)
+        else:
+            assert general[np.float64] == general[np.float32], (w, lv, general)
+    assert _lib.load().lifted_device_check(torch.cuda.current_stream().cuda_stream) == 0
