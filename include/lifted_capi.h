@@ -385,7 +385,17 @@ LIFTED_CAPI uint64_t lifted_kernel_launch_count(const char* family);
  *   "batch_nd_mode"        0..2 batches of nD images: 0 automatic, 1 one
  *                               persistent launch of line items, 2 one
  *                               separable call per group of identically
- *                               shaped, packed images */
+ *                               shaped, packed images
+ *   "zero_step_code"       0/1  Zero-boundary passes on the general line
+ *                               kernel and the batch engine's whole and
+ *                               line items sum each update's in-band taps
+ *                               directly (same results; else the exact
+ *                               step code with its boundary map)
+ *   "edge_kernels_always"  0/1  Zero passes run the exact-edge kernel
+ *                               instantiations too (for comparing them)
+ *   "overlap_in_graphs"    0..2 programmatic dependent launch inside
+ *                               stream captures: 0 never, 1 always, 2 the
+ *                               TMA-staged strided kernel only */
 LIFTED_CAPI int lifted_set_option(const char* name, int64_t value);
 /* Synchronises `stream` and reports LIFTED_ETIMEOUT if a kernel of this
  * library gave up a bounded device-side wait since the last check (the

@@ -69,7 +69,9 @@ struct BatchItem {
   int32_t wait_target;  // value that counter must reach
   int32_t done_ctr;     // counter this item increments when done (-1: none)
   int32_t geo;          // line items: index of the axis pass's geometry
-  int32_t pad_;
+  int32_t zfast;        // whole and line items: 1 = Zero boundary, direct
+                        // step code (zero_step), the host having checked
+                        // that no level's edge ranges overlap
   int64_t n0;           // signal length (line items: line length)
   int64_t in_off;       // signal offset in `in` (elements)
   int64_t out_off;      // signal offset in `out`

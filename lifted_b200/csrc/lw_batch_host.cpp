@@ -295,6 +295,7 @@ int plan_create(uint32_t op, uint32_t bc, size_t nsig,
       it.kind = fwd ? BI_WHOLE_FWD : BI_WHOLE_REV;
       it.lev0 = 0;
       it.nlev = (int32_t)L;
+      it.zfast = zero_fast_ok(dprogs[pi], (int)bc, m[0], (int)L) ? 1 : 0;
       it.src_sel = BS_IN;
       it.src_off = base.in_off;
       it.dst_sel = BS_OUT;
@@ -382,6 +383,7 @@ int plan_create(uint32_t op, uint32_t bc, size_t nsig,
         it.kind = BI_WHOLE_FWD;
         it.lev0 = (int32_t)lw;
         it.nlev = (int32_t)(L - lw);
+        it.zfast = zero_fast_ok(dprogs[pi], (int)bc, m[lw], (int)(L - lw)) ? 1 : 0;
         it.src_sel = BS_SCRATCH;
         it.src_off = band_off[(int)lw];
         it.dst_sel = BS_OUT;
@@ -398,6 +400,7 @@ int plan_create(uint32_t op, uint32_t bc, size_t nsig,
         it.kind = BI_WHOLE_REV;
         it.lev0 = (int32_t)lw;
         it.nlev = (int32_t)(L - lw);
+        it.zfast = zero_fast_ok(dprogs[pi], (int)bc, m[lw], (int)(L - lw)) ? 1 : 0;
         it.src_sel = BS_IN;
         it.src_off = base.in_off;
         it.dst_sel = BS_SCRATCH;
@@ -897,6 +900,7 @@ int plan_create_nd(uint32_t op, uint32_t bc, size_t nimg, const lifted_image_t* 
       if (nit > (int64_t)INT32_MAX / 2 || (int64_t)items.size() + nit > (int64_t)INT32_MAX / 2)
         return set_error(LIFTED_EINVAL, "image %zu: too many line items", ii);
       const int32_t ctr = k + 1 < run.size() ? nctr++ : -1;
+      const int32_t zf = zero_fast_ok(dprogs[pi], (int)bc, n, (int)lv[a]) ? 1 : 0;
       for (int64_t t = 0; t < nit; ++t) {
         BatchItem it;
         std::memset(&it, 0, sizeof(it));
@@ -911,6 +915,7 @@ int plan_create_nd(uint32_t op, uint32_t bc, size_t nimg, const lifted_image_t* 
         it.wait_target = prev_n;
         it.done_ctr = ctr;
         it.geo = gi;
+        it.zfast = zf;
         it.n0 = n;
         it.in_off = (int64_t)im.in_offset;
         it.out_off = (int64_t)im.out_offset;

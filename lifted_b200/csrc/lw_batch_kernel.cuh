@@ -321,8 +321,8 @@ __device__ void whole_fwd(const BatchParams<T>& p, const BatchItem& w,
       A[(i & 1) ? ns + (i >> 1) : (i >> 1)] = ld_band(w.src_sel, src + i);
   }
   __syncthreads();
-  run_program(prog, bc, A, m, 1, ns, nd);
-  if (w.nlev > 1) coarse_forward(prog, bc, A, m, B, ns, 1, ns, w.nlev - 1);
+  run_program_sel(prog, bc, w.zfast != 0, A, m, 1, ns, nd);
+  if (w.nlev > 1) coarse_forward(prog, bc, A, m, B, ns, 1, ns, w.nlev - 1, w.zfast != 0);
   T* dst = p.out + w.out_off;
   for (int64_t i = tid; i < m; i += nth) dst[i] = A[i];
 }
@@ -345,8 +345,8 @@ __device__ void whole_rev(const BatchParams<T>& p, const BatchItem& w,
     for (int64_t i = tid; i < m; i += nth) A[i] = __ldg(src + i);
   }
   __syncthreads();
-  if (w.nlev > 1) coarse_reverse(prog, bc, A, m, B, ns, 1, ns, w.nlev - 1);
-  run_program(prog, bc, A, m, 1, ns, nd);
+  if (w.nlev > 1) coarse_reverse(prog, bc, A, m, B, ns, 1, ns, w.nlev - 1, w.zfast != 0);
+  run_program_sel(prog, bc, w.zfast != 0, A, m, 1, ns, nd);
   T* dst = band_ptr_w(p, w.dst_sel, w.dst_off);
   for (int64_t i = tid; i < m; i += nth)
     dst[i] = A[(i & 1) ? ns + (i >> 1) : (i >> 1)];
@@ -401,8 +401,8 @@ __device__ void lines_fwd(const BatchParams<T>& p, const BatchItem& w,
   }
   if (smem) cp_wait();
   __syncthreads();
-  run_program(prog, bc, A, n, W, ns, nd);
-  if (w.nlev > 1) coarse_forward(prog, bc, A, n, B, ns, W, ns, w.nlev - 1);
+  run_program_sel(prog, bc, w.zfast != 0, A, n, W, ns, nd);
+  if (w.nlev > 1) coarse_forward(prog, bc, A, n, B, ns, W, ns, w.nlev - 1, w.zfast != 0);
   T* dst = p.out + w.out_off;
   for (int64_t f = tid; f < tot; f += nth) {
     int j;
@@ -439,8 +439,8 @@ __device__ void lines_rev(const BatchParams<T>& p, const BatchItem& w,
   }
   if (smem) cp_wait();
   __syncthreads();
-  if (w.nlev > 1) coarse_reverse(prog, bc, A, n, B, ns, W, ns, w.nlev - 1);
-  run_program(prog, bc, A, n, W, ns, nd);
+  if (w.nlev > 1) coarse_reverse(prog, bc, A, n, B, ns, W, ns, w.nlev - 1, w.zfast != 0);
+  run_program_sel(prog, bc, w.zfast != 0, A, n, W, ns, nd);
   T* dst = p.out + w.out_off;
   for (int64_t f = tid; f < tot; f += nth) {
     int j;

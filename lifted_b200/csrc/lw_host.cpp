@@ -88,6 +88,7 @@ std::atomic<int64_t> g_opt_col_row_order{1};
 std::atomic<int64_t> g_opt_batch_nd_mode{0};
 std::atomic<int64_t> g_opt_edge_always{0};
 std::atomic<int64_t> g_opt_overlap_graphs{0};
+std::atomic<int64_t> g_opt_zero_steps{1};
 
 }  // namespace
 
@@ -406,6 +407,7 @@ int run_axis_pass(const Program& prog, int op, int bc, int across,
   p.levels = (int32_t)levels;
   p.bc = bc;
   resolve_program<T>(prog, op, across, &p.prog);
+  p.zfast = zero_fast_ok(p.prog, bc, g.n, (int)levels) ? 1 : 0;
 
   if (opt.fast_path && !opt.force_global && !opt.no_alloc) {
     // Overlap of source and destination spans (in place, or aliasing).
@@ -550,6 +552,27 @@ int copy_strided(size_t ndim, const int64_t* shape, const int64_t* sin,
 }
 
 }  // namespace
+
+template <typename T>
+bool zero_fast_ok(const DevProgram<T>& prog, int bc, int64_t n, int levels) {
+  if (bc != BC_ZERO || !g_opt_zero_steps.load()) return false;
+  int64_t m = n;
+  for (int l = 0; l < levels; ++l) {
+    const int64_t nd = m / 2, ns = m - nd;
+    for (int k = 0; k < prog.nsteps; ++k) {
+      const DevStep<T>& st = prog.st[k];
+      if (st.kind == K_SCALE) continue;
+      const int64_t ny = st.y_is_d ? nd : ns;
+      const int64_t n1 = std::min<int64_t>(st.nf, ny);
+      const int64_t n2 = nd > st.nb ? nd - st.nb : 0;
+      if (n1 > n2) return false;
+    }
+    m = ns;
+  }
+  return true;
+}
+template bool zero_fast_ok<float>(const DevProgram<float>&, int, int64_t, int);
+template bool zero_fast_ok<double>(const DevProgram<double>&, int, int64_t, int);
 
 // Validation shared by both drivers.
 int check_common(uint32_t op, uint32_t bc, size_t ndim, const size_t* shape,
@@ -869,6 +892,8 @@ int set_option(const char* name, int64_t value) {
   } else if (!std::strcmp(name, "overlap_in_graphs")) {
     if (value < 0 || value > 2) return set_error(LIFTED_EINVAL, "overlap_in_graphs outside 0..2");
     g_opt_overlap_graphs = value;
+  } else if (!std::strcmp(name, "zero_step_code")) {
+    g_opt_zero_steps = value ? 1 : 0;
   } else if (!std::strcmp(name, "edge_kernels_always")) {
     g_opt_edge_always = value ? 1 : 0;
   } else if (!std::strcmp(name, "batch_nd_mode")) {

@@ -93,6 +93,14 @@ int batch_nd_mode();
 // instantiations too (their edge work then never runs; for comparing the
 // two instantiations).
 bool edge_kernels_always();
+// Whether zero_step (lw_line_kernel.cuh) reproduces the exact step code on
+// `levels` levels of a line of length n under boundary bc: the Zero boundary
+// and, at every level (bands of ceil(m / 2) and floor(m / 2)), no step whose
+// front edge range [0, n1) reaches past the start n2 of its back edge range
+// (src/lifted-steps-inl.hpp:409-410; such indices take both updates).
+// False as well when the "zero_step_code" option is off.
+template <typename T>
+bool zero_fast_ok(const DevProgram<T>& prog, int bc, int64_t n, int levels);
 // Per-axis levels of the separable driver, resolved and checked (level 0 =
 // max_level; degenerate bands refused), as lifted_lwt_sep_* does.
 int resolve_sep_levels(const Program& prog, uint32_t op, uint32_t bc,

@@ -300,6 +300,70 @@ __device__ __forceinline__ void run_program(const DevProgram<T>& prog, int bc,
     run_step(prog.st[k], prog.normal, prog.across, bc, A, pitch, W, ns, nd);
 }
 
+// One step over W lines held as in run_step, Zero boundary, on bands where
+// no step's front edge range [0, n1) reaches past the start n2 of its back
+// edge range (the host checks every level: zero_fast_ok).  There run_step
+// gives every index of y one update, whose sum runs over the taps inside the
+// source band in tap order (the front and back loops through the Zero map,
+// which drops the others; the interior loop, whose taps are all inside), in
+// both directions: the Zero boundary's adjoint folds change nothing.  This
+// computes that sum directly, without the boundary map or the partition.
+template <typename T>
+__device__ void zero_step(const DevStep<T>& st, T* A, int64_t pitch, int W,
+                          int64_t ns, int64_t nd) {
+  const int tid = threadIdx.x;
+  const int nth = blockDim.x;
+  if (st.kind == K_SCALE) {
+    const int64_t m = ns + nd;
+    const int64_t tot = (int64_t)W * m;
+    for (int64_t f = tid; f < tot; f += nth) {
+      int j;
+      int64_t i;
+      split_index(f, m, W, j, i);
+      T* p = A + j * pitch + i;
+      *p = *p * (i < ns ? st.sm : st.dm);
+    }
+    return;
+  }
+  const int64_t nx = st.y_is_d ? ns : nd;
+  const int64_t ny = st.y_is_d ? nd : ns;
+  const int64_t xo = st.y_is_d ? 0 : ns;
+  const int64_t yo = st.y_is_d ? ns : 0;
+  const int64_t tot = (int64_t)W * ny;
+  for (int64_t f = tid; f < tot; f += nth) {
+    int j;
+    int64_t i;
+    split_index(f, ny, W, j, i);
+    T* line = A + j * pitch;
+    const T* x = line + xo;
+    const int64_t b = i + st.off;
+    T y = line[yo + i];
+    if (st.kind == K_UNIT) {
+      if (b >= 0 && b < nx) y = st.sub ? y - x[b] : y + x[b];
+    } else if (b >= 0 && b + st.ntaps <= nx) {
+      y = ip_interior(st, y, x, i);
+    } else {
+      y = ip_safe(st, y, x, b, nx);
+    }
+    line[yo + i] = y;
+  }
+}
+
+// The step program on W lines: the exact step code, or (zf) zero_step.
+template <typename T>
+__device__ __forceinline__ void run_program_sel(const DevProgram<T>& prog, int bc, bool zf,
+                                                T* A, int64_t pitch, int W,
+                                                int64_t ns, int64_t nd) {
+  if (!zf) {
+    run_program(prog, bc, A, pitch, W, ns, nd);
+    return;
+  }
+  for (int k = 0; k < prog.nsteps; ++k) {
+    zero_step(prog.st[k], A, pitch, W, ns, nd);
+    __syncthreads();
+  }
+}
+
 // Forward-stepping levels on W lines held raw (not yet split) at
 // A + j * pitch, length m each (B needs m elements per line): every level splits A[0..m) into
 // [evens | odds] through B (src/lifted-ops-inl.hpp:104-135), runs the steps
@@ -308,7 +372,7 @@ __device__ __forceinline__ void run_program(const DevProgram<T>& prog, int bc,
 template <typename T>
 __device__ void coarse_forward(const DevProgram<T>& prog, int bc, T* A,
                                int64_t pitch, T* B, int64_t pitch_b, int W,
-                               int64_t m, int nlev) {
+                               int64_t m, int nlev, bool zf = false) {
   const int tid = threadIdx.x;
   const int nth = blockDim.x;
   for (int lvl = 0; lvl < nlev; ++lvl) {
@@ -328,7 +392,7 @@ __device__ void coarse_forward(const DevProgram<T>& prog, int bc, T* A,
       A[j * pitch + ((i & 1) ? ns + (i >> 1) : (i >> 1))] = B[j * pitch_b + i];
     }
     __syncthreads();
-    run_program(prog, bc, A, pitch, W, ns, nd);
+    run_program_sel(prog, bc, zf, A, pitch, W, ns, nd);
     m = ns;
   }
 }
@@ -341,7 +405,7 @@ __device__ void coarse_forward(const DevProgram<T>& prog, int bc, T* A,
 template <typename T>
 __device__ void coarse_reverse(const DevProgram<T>& prog, int bc, T* A,
                                int64_t pitch, T* B, int64_t pitch_b, int W,
-                               int64_t m0, int nlev) {
+                               int64_t m0, int nlev, bool zf = false) {
   const int tid = threadIdx.x;
   const int nth = blockDim.x;
   int64_t msz[MAX_LEVELS + 1];
@@ -350,7 +414,7 @@ __device__ void coarse_reverse(const DevProgram<T>& prog, int bc, T* A,
   for (int lvl = nlev - 1; lvl >= 0; --lvl) {
     const int64_t m = msz[lvl];
     const int64_t nd = m / 2, ns = m - nd;
-    run_program(prog, bc, A, pitch, W, ns, nd);
+    run_program_sel(prog, bc, zf, A, pitch, W, ns, nd);
     const int64_t t2 = (int64_t)W * m;
     for (int64_t f = tid; f < t2; f += nth) {
       int j;
@@ -453,7 +517,7 @@ __global__ void __launch_bounds__(512)
           }
           __syncthreads();
         }
-        run_program(p.prog, p.bc, A, p.pitch, We, ns, nd);
+        run_program_sel(p.prog, p.bc, p.zfast != 0, A, p.pitch, We, ns, nd);
         m = ns;
       }
       // A now holds [a_L | d_L | ... | d_1] (Q11).
@@ -478,7 +542,7 @@ __global__ void __launch_bounds__(512)
       for (int lvl = p.levels - 1; lvl >= 0; --lvl) {
         const int64_t m = msz[lvl];
         const int64_t nd = m / 2, ns = m - nd;
-        run_program(p.prog, p.bc, A, p.pitch, We, ns, nd);
+        run_program_sel(p.prog, p.bc, p.zfast != 0, A, p.pitch, We, ns, nd);
         if (lvl > 0) {
           const int64_t t2 = (int64_t)We * m;
           for (int64_t f = tid; f < t2; f += nth) {

@@ -90,6 +90,8 @@ struct LineParams {
   int32_t bc;
   int32_t W;          // lines per CTA
   int32_t use_smem;   // 1: buffers in dynamic shared memory
+  int32_t zfast;      // 1: Zero boundary, direct step code (zero_step)
+  int32_t pad_;
   int64_t pitch;      // elements per line in buffer A
   int64_t pitch_b;    // elements per line in buffer B
   T* scratch;         // global buffers when use_smem == 0
