@@ -498,6 +498,53 @@ def generic_section(dev, steps: int = 10):
     return out
 
 
+def odd_section(dev, steps: int = 5):
+    """Odd extents (bands of ceil(m / 2) and floor(m / 2)), which the
+    register kernels do not take: 4095^2 float32 CDF 9/7 levels (6, 6),
+    Forward + ForwardAdjoint, graph-replayed, on the general line kernel with
+    the direct Zero-boundary step code and with the exact step code (option
+    off) beside it."""
+    import torch
+    from lifted_b200 import _lib
+    from lifted_b200 import pylifted as pl
+
+    g = torch.Generator(device=dev).manual_seed(1008)
+    x = torch.randn(4095, 4095, device=dev, generator=g)
+    w = torch.empty_like(x)
+    y = torch.empty_like(x)
+    B = 2 * 2 * x.numel() * 4
+    out = {"workload": "4095^2 float32 N(0,1) (seed 1008), CDF 9/7 levels (6, 6) on axes "
+                       "(0, 1), Zero boundary, Forward + ForwardAdjoint", "unit": "GB/s"}
+    for on in (1, 0):
+        _lib.set_option("zero_step_code", on)
+        try:
+            def step():
+                pl._lwt(x, WAVELET, 0, 0, (0, 1), (6, 6), 1, out=w)
+                pl._lwt(w, WAVELET, 0, 2, (0, 1), (6, 6), 1, out=y)
+
+            for _ in range(2):
+                step()
+            torch.cuda.synchronize(dev)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+                step()
+            graph.replay()
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                graph.replay()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1) / steps
+            key = "direct_zero_steps" if on else "exact_steps"
+            out[key] = {"value": round(B / ms / 1e6, 3), "ms_per_step": round(ms, 4)}
+            del graph
+        finally:
+            _lib.set_option("zero_step_code", 1)
+    return out
+
+
 def inverse_section(dev, x, steps: int = 10):
     """Inverse + InverseAdjoint of the headline workload (the same kernels
     with the step order and signs of those transforms), timed as a CUDA
@@ -771,7 +818,7 @@ def main() -> int:
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched, autograd and least-squares sections")
     ap.add_argument("--section", choices=["inverse", "cfg1", "batched", "batched_nd", "autograd",
-                                          "lsq", "generic", "boundaries"],
+                                          "lsq", "generic", "boundaries", "odd"],
                     help="run only this section (one GPU) and print its JSON; for profiling "
                          "its kernels, not a driver line")
     args = ap.parse_args()
@@ -797,6 +844,7 @@ def main() -> int:
         else:
             fn = {"cfg1": cfg1_section, "batched": batched_section,
                   "batched_nd": batched_nd_section, "generic": generic_section,
+                  "odd": odd_section,
                   "autograd": autograd_section, "lsq": lsq_section}[args.section]
             res = fn(dev)
         print(json.dumps({"section": args.section, **res}))
@@ -981,7 +1029,7 @@ def main() -> int:
                              f"{cores} threads)"}
 
     extras = {"inverse": None, "cfg1_1d_f64": None, "batched": None, "batched_nd": None,
-              "autograd": None, "lsq": None, "generic": None, "boundaries": None}
+              "autograd": None, "lsq": None, "generic": None, "boundaries": None, "odd": None}
     if world == 1 and not args.no_extras:
         extras["inverse"] = inverse_section(dev, x)
         extras["boundaries"] = boundaries_section(dev, x)
@@ -991,6 +1039,7 @@ def main() -> int:
         extras["autograd"] = autograd_section(dev)
         extras["lsq"] = lsq_section(dev)
         extras["generic"] = generic_section(dev)
+        extras["odd"] = odd_section(dev)
 
     if world > 1:
         dist.barrier()
@@ -1027,6 +1076,7 @@ def main() -> int:
             "batched": extras["batched"],
             "batched_nd": extras["batched_nd"],
             "generic_wavelets": extras["generic"],
+            "odd_extents": extras["odd"],
             "boundaries": extras["boundaries"],
             "autograd": extras["autograd"],
             "lsq": extras["lsq"],
