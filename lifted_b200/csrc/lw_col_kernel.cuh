@@ -179,7 +179,8 @@ __device__ __forceinline__ void issue(const ColParams<T>& p, int64_t t, T* stage
     const int k = p.r.nreg;
     int row = 0;
     for (int l = 1; l <= k; ++l) {
-      const int64_t ml = p.r.g.n >> l;
+      // d_l starts at ceil(n / 2^l)
+      const int64_t ml = (p.r.g.n + ((int64_t)1 << l) - 1) >> l;
       tma_box(stage + (size_t)row * W, &p.tm_rows[l - 1], x, (int)(ml + (tc.wstart >> l)), z,
               r3, bar, pol);
       row += COL_ROWS >> l;
@@ -243,6 +244,7 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
         const RegParams<T>& p = *c.p;
         const int64_t nb = c.n >> (LV + 1);
         const int64_t gp0 = c.e0 >> (LV + 1);
+        if constexpr (EM) reg::level_lengths(c, LV);
         if (LV + 1 == k && (LV > 0 || !preload_d1<T>()))
           read_rows<T, VT, V, P, P0>(s, rs.stage, region_row(k) + c.r * P, c.j);
         if constexpr (LV > 0 || !preload_d1<T>()) {
@@ -261,15 +263,14 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
         if constexpr (LV == 0) {
           if (reg::chunk_stored(c)) {
             T* o = p.out + c.bout + c.e0 * p.g.sout;
-            // EM: the line may end inside this chunk
-            const int64_t rem = nb - gp0;
-            const int lim = !EM ? P : (rem >= P ? P : (rem > 0 ? (int)rem : 0));
+            // EM: the line may end inside this chunk, after an s value
+            // (odd length)
+            const int lim_s = !EM ? P : reg::chunk_lim(c.nsl, gp0, P);
+            const int lim_d = !EM ? P : reg::chunk_lim(c.ndl, gp0, P);
 #pragma unroll
             for (int i = 0; i < P; ++i) {
-              if (!EM || i < lim) {
-                st_hint(o + (2 * i) * p.g.sout, s[i], c.pol_st);
-                st_hint(o + (2 * i + 1) * p.g.sout, d[i], c.pol_st);
-              }
+              if (!EM || i < lim_s) st_hint(o + (2 * i) * p.g.sout, s[i], c.pol_st);
+              if (!EM || i < lim_d) st_hint(o + (2 * i + 1) * p.g.sout, d[i], c.pol_st);
             }
           }
         } else {

@@ -211,6 +211,8 @@ struct Ctx {
   bool has_l, has_r, line_ok;
   int64_t L, bin, bout, n, e0, tile_lo, tile_hi;
   int buf;
+  int64_t nsl, ndl; // band lengths of the current level: s (ceil(m / 2)) and
+                    // d (floor(m / 2)) of the level's input band of m
   int mb_bufs;      // mailbox buffers: 2 (alternating, one barrier per
                     // step) or 1 (a second barrier after the reads)
   int bc;           // boundary condition of the pass
@@ -237,14 +239,18 @@ __device__ __forceinline__ VT tap(const VT* xl, const bool* vl, const VT* x,
 // band (nb pairs) may end inside a chunk (lines whose length is not a
 // multiple of the chunk); in-chunk taps past the end are skipped.
 template <typename T, typename VT, int P, int PA, int HMAX, int KIND, int OFF,
-          int NT, int SUB, int HL, int HR, bool EM = false, bool EDGE = false>
+          int NT, int SUB, int HL, int HR, bool YD, bool EM = false, bool EDGE = false>
 __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
                                        const DevStep<T>& st, Ctx<T>& c,
                                        int64_t gp0, int64_t nb) {
   static_assert(HL <= P && HR <= P, "step reaches past the neighbour chunk");
+  // taps count inside the source band: s (YD: y is d) or d, which differ in
+  // length by one on a band of odd length
   int lim = P;
+  int64_t nx = nb;
   if constexpr (EM) {
-    const int64_t rem = nb - gp0;
+    nx = YD ? c.nsl : c.ndl;
+    const int64_t rem = nx - gp0;
     lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
   }
   // Constant / Symmetric / Reflect: the chunks holding a band end redo
@@ -279,7 +285,7 @@ __device__ __forceinline__ void update(VT (&y)[PA], const VT (&x)[PA],
 #pragma unroll
   for (int h = 0; h < HR; ++h) {
     xr[h] = c.has_r ? mb_first[h * nth + c.tid_r] : vzero<VT>();
-    vr[h] = (gp0 + P + h) < nb;
+    vr[h] = (gp0 + P + h) < nx;
   }
   if (c.mb_bufs == 1) __syncthreads();  // the mailbox is read before the next step writes it
 #pragma unroll
@@ -329,11 +335,11 @@ __device__ __forceinline__ void gen_update(int shape, VT (&s)[PA], VT (&d)[PA],
       constexpr CStep cs = GenTable<OP>::v.s[I];
       if constexpr (cs.left <= P && cs.right <= P && cs.left <= HMAX && cs.right <= HMAX) {
         if constexpr (cs.y_is_d)
-          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(
-              d, s, st, c, gp0, nb);
+          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, true,
+                 EM>(d, s, st, c, gp0, nb);
         else
-          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, EM>(
-              s, d, st, c, gp0, nb);
+          update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left, cs.right, false,
+                 EM>(s, d, st, c, gp0, nb);
       }
       return;
     }
@@ -374,10 +380,10 @@ __device__ __forceinline__ void steps(VT (&s)[PA], VT (&d)[PA], Ctx<T>& c,
       }
     } else if constexpr (cs.y_is_d) {
       update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
-             cs.right, EM, EDGE>(d, s, st, c, gp0, nb);
+             cs.right, true, EM, EDGE>(d, s, st, c, gp0, nb);
     } else {
       update<T, VT, P, PA, HMAX, cs.kind, cs.off, cs.ntaps, cs.sub, cs.left,
-             cs.right, EM, EDGE>(s, d, st, c, gp0, nb);
+             cs.right, false, EM, EDGE>(s, d, st, c, gp0, nb);
     }
     steps<T, VT, WI, OP, K + 1, P, PA, HMAX, EM, EDGE>(s, d, c, gp0, nb);
   }
@@ -446,9 +452,24 @@ __device__ __forceinline__ bool chunk_stored(const Ctx<T>& c) {
   return c.line_ok && c.e0 >= c.tile_lo && c.e0 < c.tile_hi;
 }
 
+// Band lengths of level lv of a line of n samples: its input band has
+// ceil(n / 2^lv) samples, split into ceil and floor halves.
+template <typename T>
+__device__ __forceinline__ void level_lengths(Ctx<T>& c, int lv) {
+  const int64_t m = (c.n + ((int64_t)1 << lv) - 1) >> lv;
+  c.ndl = m >> 1;
+  c.nsl = m - c.ndl;
+}
+
+__device__ __forceinline__ int chunk_lim(int64_t len, int64_t gp0, int P) {
+  const int64_t rem = len - gp0;
+  return rem >= P ? P : (rem > 0 ? (int)rem : 0);
+}
+
 // Forward-stepping register levels (Forward, InverseAdjoint).
-// EM: lines whose length is a multiple of 2^levels but not of the chunk;
-// the band ends inside a chunk, whose stores stop there.
+// EM: lines whose length is not a multiple of the chunk: a band ends inside
+// a chunk, whose stores stop there; at a level whose input band is odd the
+// s band is one longer than the d band.
 template <typename T, typename VT, int V, int WI, int OP, int P0, int HMAX,
           int LV, bool TILE, bool EM = false, bool EDGE = false>
 __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
@@ -458,14 +479,14 @@ __device__ __forceinline__ void fwd_levels(VT (&s)[P0], VT (&d)[P0],
     if (LV < c.p->nreg) {
       const int64_t nb = c.n >> (LV + 1);
       const int64_t gp0 = c.e0 >> (LV + 1);
-      int lim = P;
+      int lim = P;  // s values of this chunk inside the band
       if constexpr (EM) {
-        const int64_t rem = nb - gp0;
-        lim = rem >= P ? P : (rem > 0 ? (int)rem : 0);
+        level_lengths(c, LV);
+        lim = chunk_lim(c.nsl, gp0, P);
       }
       steps_sel<T, VT, WI, OP, P, P0, HMAX, EM, EDGE>(s, d, c, gp0, nb);
       if (chunk_stored(c)) {
-        if constexpr (EM) store_first<T, VT, P, P0>(d, c, nb + gp0, lim);
+        if constexpr (EM) store_first<T, VT, P, P0>(d, c, c.nsl + gp0, chunk_lim(c.ndl, gp0, P));
         else store_run<T, VT, P, P0>(d, c, nb + gp0);
       }
       if (LV + 1 == c.p->nreg) {

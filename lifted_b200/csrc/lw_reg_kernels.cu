@@ -78,18 +78,24 @@ bool set_gen_shapes(DevProgram<T>* p, int op) {
 // Bands of n >> (l + 1) pairs (every level's band a whole number of pairs).
 template <typename T>
 bool edges_overlap(const DevProgram<T>& prog, int64_t n, int levels) {
+  int64_t m = n;  // the level's input band: s of ceil(m / 2), d of floor(m / 2)
   for (int l = 0; l < levels; ++l) {
-    const int64_t ny = n >> (l + 1);
+    const int64_t nd = m / 2, ns = m - nd;
     for (int k = 0; k < prog.nsteps; ++k) {
       const DevStep<T>& st = prog.st[k];
       if (st.kind == K_SCALE) continue;
+      const int64_t ny = st.y_is_d ? nd : ns;
       const int64_t n1 = st.nf < ny ? (int64_t)st.nf : ny;
-      const int64_t n2 = ny > st.nb ? ny - st.nb : 0;
+      const int64_t n2 = nd > st.nb ? nd - st.nb : 0;
       if (n1 > n2) return true;
     }
+    m = ns;
   }
   return false;
 }
+
+// Length of the approximation band after k levels: ceil(n / 2^k).
+inline int64_t band_after(int64_t n, int k) { return (n + ((int64_t)1 << k) - 1) >> k; }
 
 // How far from a band end (pairs) the exact edge work of the register
 // kernels reaches under boundary bc (lw_edge.cuh): the largest distance from
@@ -654,14 +660,14 @@ bool col_levels_plan(int wi, int op, int64_t n, int levels, int F, int* k_out, i
     // again, which needs band lines a multiple of 32 long (float64 lines
     // of 512 with more levels than the registers hold)
     if (levels > k && n / (2 * p0_of<T>()) > 16)
-      while (k > 0 && ((n >> k) % 32)) --k;
+      while (k > 0 && (band_after(n, k) % 32)) --k;
     *tile = n;
     *halo = 0;
     *ntr = 1;
   } else {
     for (int kk = 1; kk <= maxreg && kk <= levels; ++kk) {
       k = kk;
-      const int64_t m = n >> kk;
+      const int64_t m = band_after(n, kk);
       if (m % 32 == 0 && m / 32 <= 16) break;
     }
     int64_t need = 0;
@@ -683,14 +689,15 @@ bool col_levels_plan(int wi, int op, int64_t n, int levels, int F, int* k_out, i
 // before the first launch, so no launch is left without its band pass.
 template <typename T>
 bool col_chain_ok(int wi, int op, int64_t n, int levels, int F, int depth) {
-  // lines a multiple of 32 long, or of 2^levels (the band ends inside a
-  // chunk: the end-masked instantiation)
-  if (depth > 8 || (n % 32 && n % ((int64_t)1 << levels))) return false;
+  // lines a multiple of 32 long, or (the end-masked instantiation: a band
+  // ends inside a chunk) of any length under the Zero boundary (F == 1),
+  // else of a multiple of 2^levels
+  if (depth > 8 || (n % 32 && F != 1 && n % ((int64_t)1 << levels))) return false;
   int k;
   int64_t tile, halo, ntr;
   if (!col_levels_plan<T>(wi, op, n, levels, F, &k, &tile, &halo, &ntr)) return false;
   if (levels == k) return true;
-  const int64_t m = n >> k;
+  const int64_t m = band_after(n, k);
   if (col_chain_ok<T>(wi, op, m, levels - k, F, depth + 1)) return true;
   constexpr int P0 = p0_of<T>();
   return compiled_wavelet(wi) && m % (2 * P0) == 0 && m / (2 * P0) <= 16 &&
@@ -718,10 +725,10 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if (g.nother == 2 && (g.oin[1] <= 0 || ((g.oin[1] * EB) & 15))) return 0;
     if (!aligned16(a.in)) return 0;
     const int64_t n = g.n;
-    // lines whose length is a multiple of 2^levels but not of 32: the
-    // end-masked instantiation, one line per lane
+    // lines whose length is not a multiple of 32: the end-masked
+    // instantiation, one line per lane (Zero boundary, any length: bands of
+    // odd length at some level have an s band one longer than the d band)
     const bool em = (n % 32) != 0;
-    if (em && n % ((int64_t)1 << a.levels)) return 0;
     // exact band edges of the non-Zero boundaries need whole chunks
     const int F = edge_footprint(*a.prog, a.bc);
     if (F < 0 || (em && a.bc != BC_ZERO)) return 0;
@@ -767,7 +774,7 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v, em, edge_inst);
     else fn = pick_col_f64(wk, op, em, edge_inst);
     if (!fn) return 0;
-    const int64_t m = n >> k;
+    const int64_t m = band_after(n, k);
     const bool more = a.levels > k;
     if (more && !col_chain_ok<T>(wi, op, n, a.levels, F, 0)) return 0;
     if (!more && a.levels != k) return 0;
