@@ -1,6 +1,7 @@
 // Instantiation helpers of the TMA-staged strided kernel (lw_col_kernel.cuh),
 // shared by the translation units that instantiate it (lw_col_f32.cu,
-// lw_col_f64.cu, lw_col_edge.cu: split so that they compile in parallel).
+// lw_col_f64.cu, lw_col_edge.cu, lw_col_ldg.cu: split so that they compile
+// in parallel).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -14,9 +15,9 @@ namespace lw {
 namespace colinst {
 
 
-template <typename T, int WI, int OP, int V, bool EM, bool EDGE>
+template <typename T, int WI, int OP, int V, bool EM, bool EDGE, bool LDG = false>
 cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_t stream) {
-  auto kern = col_kernel<T, WI, OP, V, EM, EDGE>;
+  auto kern = col_kernel<T, WI, OP, V, EM, EDGE, LDG>;
   static bool configured[kMaxDevices] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -31,13 +32,13 @@ cudaError_t launch_one(const ColParams<T>& p, int grid, size_t smem, cudaStream_
   return launch_overlapped_kind(1, kern, grid, COL_THREADS, smem, stream, p);
 }
 
-template <typename T, int WI, int V, bool EM, bool EDGE = false>
+template <typename T, int WI, int V, bool EM, bool EDGE = false, bool LDG = false>
 ColFn<T> by_op(int op) {
   switch (op) {
-    case 0: return launch_one<T, WI, 0, V, EM, EDGE>;
-    case 1: return launch_one<T, WI, 1, V, EM, EDGE>;
-    case 2: return launch_one<T, WI, 2, V, EM, EDGE>;
-    default: return launch_one<T, WI, 3, V, EM, EDGE>;
+    case 0: return launch_one<T, WI, 0, V, EM, EDGE, LDG>;
+    case 1: return launch_one<T, WI, 1, V, EM, EDGE, LDG>;
+    case 2: return launch_one<T, WI, 2, V, EM, EDGE, LDG>;
+    default: return launch_one<T, WI, 3, V, EM, EDGE, LDG>;
   }
 }
 
@@ -53,15 +54,15 @@ ColFn<T> edge_wavelet(int wi, int op) {
   }
 }
 
-template <typename T, int V, bool EM>
+template <typename T, int V, bool EM, bool LDG = false>
 ColFn<T> by_wavelet(int wi, int op) {
   switch (wi) {
-    case 2: return by_op<T, 2, V, EM>(op);
-    case 4: return by_op<T, 4, V, EM>(op);
-    case 33: return by_op<T, 33, V, EM>(op);
-    case WI_GEN: return by_op<T, WI_GEN, V, EM>(op);
+    case 2: return by_op<T, 2, V, EM, false, LDG>(op);
+    case 4: return by_op<T, 4, V, EM, false, LDG>(op);
+    case 33: return by_op<T, 33, V, EM, false, LDG>(op);
+    case WI_GEN: return by_op<T, WI_GEN, V, EM, false, LDG>(op);
     case WI_GENW:
-      if constexpr (V == 1) return by_op<T, WI_GENW, V, EM>(op);
+      if constexpr (V == 1) return by_op<T, WI_GENW, V, EM, false, LDG>(op);
       else return nullptr;
     default: return nullptr;
   }

@@ -198,6 +198,55 @@ __device__ __forceinline__ void issue(const ColParams<T>& p, int64_t t, T* stage
   }
 }
 
+// One box of `rows` rows of 32 lanes from src (x along lines at unit stride,
+// y at stride ystr, extents xdim and ydim) into dst, zeros outside the
+// extents as the TMA's fill gives them; every thread of the CTA takes part.
+template <typename T>
+__device__ __forceinline__ void ld_box(T* dst, const T* src, int64_t xdim, int64_t ydim,
+                                       int64_t ystr, int64_t x, int64_t y, int rows) {
+  for (int e = threadIdx.x; e < rows * COL_LANES; e += COL_THREADS) {
+    const int yi = e / COL_LANES, xi = e % COL_LANES;
+    const int64_t xx = x + xi, yy = y + yi;
+    dst[e] = (xx < xdim && yy >= 0 && yy < ydim) ? src[xx + yy * ystr] : T(0);
+  }
+}
+
+// Plain-load form of issue() for lines whose stride (or line count, or
+// base) TMA cannot take (strides and the band buffer's boxes must be
+// multiples of 16 bytes): the same boxes, loaded by every thread with
+// bounds checks; one line per lane, no stacked slices.
+template <typename T, bool FWD>
+__device__ __forceinline__ void fill(const ColParams<T>& p, int64_t t, T* stage) {
+  const TileCoord tc = decode<T, 1>(p, t);
+  const LineGeom& g = p.r.g;
+  const int64_t x = tc.col0;
+  const int64_t n = g.n;
+  const bool zin = tc.outer < p.nouter;  // a z past the extent reads zeros
+  const T* in = p.r.in + (g.nother == 2 ? tc.outer * g.oin[1] : 0);
+  const int64_t xdim = zin ? p.ncols : 0;
+  if (FWD) {
+    ld_box(stage, in, xdim, n, g.sin, x, tc.wstart, COL_ROWS);
+  } else {
+    const int k = p.r.nreg;
+    int row = 0;
+    for (int l = 1; l <= k; ++l) {
+      const int64_t ml = (n + ((int64_t)1 << l) - 1) >> l;
+      ld_box(stage + (size_t)row * COL_LANES, in, xdim, n, g.sin, x, ml + (tc.wstart >> l),
+             COL_ROWS >> l);
+      row += COL_ROWS >> l;
+    }
+    if (p.a_from_tmp) {
+      // band buffer [position][line] of ceil(n / 2^k) positions
+      const int64_t m = (n + ((int64_t)1 << k) - 1) >> k;
+      ld_box(stage + (size_t)row * COL_LANES, p.r.tmp, zin ? g.nlines : 0, m, g.nlines,
+             tc.outer * p.ncols + x, tc.wstart >> k, COL_ROWS >> k);
+    } else {
+      ld_box(stage + (size_t)row * COL_LANES, in, xdim, n, g.sin, x, tc.wstart >> k,
+             COL_ROWS >> k);
+    }
+  }
+}
+
 // Per-tile state of the reverse levels: where the staged bands are and how
 // to hand the buffer back.
 template <typename T>
@@ -206,6 +255,7 @@ struct RevStage {
   uint64_t* bar;
   const ColParams<T>* p;
   int64_t next;  // next tile of this CTA (>= ntiles: none)
+  bool prefetch; // issue the next tile's copies once the buffer is free
 };
 
 // Staging row of pair 0 of this chunk in the band region of level LV
@@ -256,7 +306,7 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
         if (LV == LAST_READ) {
           // last read of the staging buffer for this tile
           __syncthreads();
-          if (c.tid == 0 && rs.next < rs.p->ntiles)
+          if (c.tid == 0 && rs.prefetch && rs.next < rs.p->ntiles)
             issue<T, false, V>(*rs.p, rs.next, const_cast<T*>(rs.stage), rs.bar);
         }
         reg::steps_sel<T, VT, WI, OP, P, P0, HMAX, EM, EDGE>(s, d, c, gp0, nb);
@@ -295,11 +345,14 @@ __device__ __forceinline__ void rev_levels(typename LaneVec<T, V>::type (&s)[P0]
 // EDGE: the instantiation for the Constant, Symmetric and Reflect
 // boundaries (exact band edges, lw_edge.cuh); Zero passes run the one
 // without that code.
-template <typename T, int WI, int OP, int V, bool EM, bool EDGE = false>
+// LDG: tiles staged by plain loads (col::fill) instead of TMA, for strides
+// TMA cannot take; no copy of the next tile runs during the levels.
+template <typename T, int WI, int OP, int V, bool EM, bool EDGE = false, bool LDG = false>
 __global__ void __launch_bounds__(COL_THREADS, 1)
     col_kernel(const __grid_constant__ ColParams<T> p) {
   using VT = typename LaneVec<T, V>::type;
   static_assert(V == 1 || sizeof(T) == 4, "packed lanes are float32 only");
+  static_assert(!LDG || V == 1, "plain-load staging takes one line per lane");
   constexpr int P0 = COL_P0;
   constexpr int W = COL_LANES * V;
   constexpr int HMAX = khmax(WI, OP);
@@ -339,9 +392,14 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
   pdl_wait();  // the previous kernel's results (no global access before)
   uint32_t parity = 0;
   int64_t t = blockIdx.x;
-  if (t < p.ntiles && tid == 0) col::issue<T, FWD, V>(p, t, stage, bar);
+  if (!LDG && t < p.ntiles && tid == 0) col::issue<T, FWD, V>(p, t, stage, bar);
   for (; t < p.ntiles; t += gridDim.x) {
     if (t + gridDim.x >= p.ntiles) pdl_trigger();  // the CTA's last tile
+    if constexpr (LDG) {
+      // the previous tile's last staging read precedes a block barrier
+      col::fill<T, FWD>(p, t, stage);
+      __syncthreads();
+    } else {
     const bool got = col::mbar_wait(bar, parity, p.spin_limit);
     if (!__syncthreads_and(got)) {
       // Give up on the tile (the host reads the flag), but do not leave
@@ -357,6 +415,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
       return;
     }
     parity ^= 1;
+    }
     const col::TileCoord tc = col::decode<T, V>(p, t);
     const int64_t outer = tc.outer + zr;
     const int64_t L = outer * p.ncols + tc.col0 + (int64_t)c.j * V;
@@ -384,7 +443,7 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
         d[i] = *reinterpret_cast<const VT*>(st + (size_t)(2 * i + 1) * W);
       }
       __syncthreads();  // staging consumed
-      if (tid == 0 && next < p.ntiles) col::issue<T, FWD, V>(p, next, stage, bar);
+      if (!LDG && tid == 0 && next < p.ntiles) col::issue<T, FWD, V>(p, next, stage, bar);
       reg::fwd_levels<T, VT, V, WI, OP, P0, HMAX, 0, true, EM, EDGE>(s, d, c);
     } else {
       const int k = p.r.nreg;
@@ -394,10 +453,10 @@ __global__ void __launch_bounds__(COL_THREADS, 1)
         if (k == 1) {
           col::read_rows<T, VT, V, P0, P0>(s, stage, col::region_row(1) + c.r * P0, c.j);
           __syncthreads();
-          if (tid == 0 && next < p.ntiles) col::issue<T, FWD, V>(p, next, stage, bar);
+          if (!LDG && tid == 0 && next < p.ntiles) col::issue<T, FWD, V>(p, next, stage, bar);
         }
       }
-      col::RevStage<T> rs{stage, bar, &p, next};
+      col::RevStage<T> rs{stage, bar, &p, next, !LDG};
       constexpr int TOP = reg_max_levels(WI, OP, P0) - 1;
       if constexpr (col::preload_d1<T>()) {
         col::rev_levels<T, WI, OP, P0, HMAX, V, TOP, EM, EDGE>(s, d, d1, c, rs);

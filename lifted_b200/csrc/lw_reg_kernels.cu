@@ -711,24 +711,30 @@ bool col_chain_ok(int wi, int op, int64_t n, int levels, int F, int depth) {
 // (band_pass).  Catalogue wavelets without compiled kernels use the generic
 // instantiations.  Returns 0 when the pass does not qualify.
 template <typename T>
-int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
+int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats,
+               bool allow_ldg) {
   {
     constexpr int EB = (int)sizeof(T);
     const LineGeom& g = a.g;
     if (!col_enabled()) return 0;
-    if (g.sin <= 1 || ((g.sin * EB) & 15)) return 0;
+    if (g.sin <= 1) return 0;
     if (!lines_adjacent(g) || g.nother > 2) return 0;
+    if (g.nother == 2 && g.oin[1] <= 0) return 0;
     const int64_t ncols = g.oshape[0];
-    // a line count that is not a multiple of 32: the last strip is partial
-    // (band-buffer boxes start at outer * ncols + col0, 16-byte aligned)
-    if (ncols % COL_LANES && (ncols < COL_LANES || ((ncols * EB) & 15))) return 0;
-    if (g.nother == 2 && (g.oin[1] <= 0 || ((g.oin[1] * EB) & 15))) return 0;
-    if (!aligned16(a.in)) return 0;
+    // TMA wants strides that are multiples of 16 bytes, a 16-byte aligned
+    // base, and (a line count that is not a multiple of 32: the last strip
+    // is partial) band-buffer boxes starting on 16 bytes at outer * ncols +
+    // col0; otherwise the plain-load instantiation stages the tiles (Zero
+    // boundary)
+    const bool ldg = ((g.sin * EB) & 15) ||
+                     (ncols % COL_LANES && (ncols < COL_LANES || ((ncols * EB) & 15))) ||
+                     (g.nother == 2 && ((g.oin[1] * EB) & 15)) || !aligned16(a.in);
+    if (ldg && (a.bc != BC_ZERO || !allow_ldg)) return 0;
     const int64_t n = g.n;
     // lines whose length is not a multiple of 32: the end-masked
     // instantiation, one line per lane (Zero boundary, any length: bands of
     // odd length at some level have an s band one longer than the d band)
-    const bool em = (n % 32) != 0;
+    const bool em = (n % 32) != 0 || ldg;
     // exact band edges of the non-Zero boundaries need whole chunks
     const int F = edge_footprint(*a.prog, a.bc);
     if (F < 0 || (em && a.bc != BC_ZERO)) return 0;
@@ -771,8 +777,10 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     // edge work overflows the registers)
     const bool edge_inst = (a.bc != BC_ZERO || edge_kernels_always()) && compiled_wavelet(wi) && !em;
     if (edge_inst) v = 1;
-    if constexpr (sizeof(T) == 4) fn = pick_col_f32(wk, op, v, em, edge_inst);
-    else fn = pick_col_f64(wk, op, em, edge_inst);
+    if constexpr (sizeof(T) == 4)
+      fn = ldg ? pick_col_ldg_f32(wk, op) : pick_col_f32(wk, op, v, em, edge_inst);
+    else
+      fn = ldg ? pick_col_ldg_f64(wk, op) : pick_col_f64(wk, op, em, edge_inst);
     if (!fn) return 0;
     const int64_t m = band_after(n, k);
     const bool more = a.levels > k;
@@ -796,7 +804,9 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
     bool ok = true;
     const cuuint32_t bx = (cuuint32_t)(COL_LANES * v);
     const bool fwd_op = (op == TF_F || op == TF_IA);
-    if (stack > 1) {
+    if (ldg) {
+      // plain-load staging: no tensor maps
+    } else if (stack > 1) {
       // forward: two boxes of stack/2 slices x n rows; reverse: region l of
       // every slice (n >> l rows) in one box of all the slices
       if (fwd_op) {
@@ -812,7 +822,8 @@ int launch_col(const RegPassArgs<T>& a, cudaStream_t stream, RegStats* stats) {
         ok = encode_rows(&cp.tm_rows[i], a.in, rank, dims, strides, bx, (cuuint32_t)(256 >> i),
                          EB);
     }
-    if (ok && more && stack > 1) {
+    if (ldg) {
+    } else if (ok && more && stack > 1) {
       // the band buffer [position][line] viewed as {line in slice, position,
       // slice}
       const cuuint64_t tdims[3] = {(cuuint64_t)ncols, (cuuint64_t)m, (cuuint64_t)nouter};
@@ -929,10 +940,18 @@ int band_pass(const RegPassArgs<T>& a, const LineGeom& g2, const T* in, T* out, 
     b.out = out;
     b.levels = levels;
     b.in_place = false;
-    const int rc = launch_col<T>(b, stream, stats);
+    const int rc = launch_col<T>(b, stream, stats, false);
     if (rc != 0) return rc;
   }
-  return launch_whole<T>(a, g2, in, out, levels, true, stream, stats);
+  const int rc = launch_whole<T>(a, g2, in, out, levels, true, stream, stats);
+  if (rc != 0 || !(g2.oin[0] == 1 && g2.oout[0] == 1)) return rc;
+  RegPassArgs<T> b = a;
+  b.g = g2;
+  b.in = in;
+  b.out = out;
+  b.levels = levels;
+  b.in_place = false;
+  return launch_col<T>(b, stream, stats, true);
 }
 
 }  // namespace
@@ -976,7 +995,7 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
       if (rc != 0) return rc;
       return launch_wtile<T>(a, stream, stats);
     }
-    if (lines_adjacent(g)) return launch_col<T>(a, stream, stats);
+    if (lines_adjacent(g)) return launch_col<T>(a, stream, stats, true);
     return 0;
   }
   // whole lines: contiguous rows, or strided lines adjacent in memory
@@ -991,11 +1010,15 @@ int plan_reg_pass(const RegPassArgs<T>& a, cudaStream_t stream,
     if (rc != 0) return rc;
   }
   if (lines_adjacent(g)) {
-    int rc = launch_col<T>(a, stream, stats);
+    // the TMA-staged form first, then the register kernels (plain loads,
+    // with their prefetch), then the plain-load form of the strided kernel
+    int rc = launch_col<T>(a, stream, stats, false);
     if (rc != 0) return rc;
     rc = launch_whole<T>(a, g, a.in, a.out, a.levels, true, stream, stats);
     if (rc != 0) return rc;
-    return launch_tiled<T>(a, stream, stats);
+    rc = launch_tiled<T>(a, stream, stats);
+    if (rc != 0) return rc;
+    return launch_col<T>(a, stream, stats, true);
   }
   return 0;
 }
