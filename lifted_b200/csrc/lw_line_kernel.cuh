@@ -330,6 +330,28 @@ __device__ void zero_step(const DevStep<T>& st, T* A, int64_t pitch, int W,
   const int64_t xo = st.y_is_d ? 0 : ns;
   const int64_t yo = st.y_is_d ? ns : 0;
   const int64_t tot = (int64_t)W * ny;
+  if (tot <= 0x7fffffffLL && nx + st.ntaps <= 0x7fffffffLL) {
+    // 32-bit positions (every shared-memory batch of lines, and any line
+    // shorter than 2^31)
+    const int nx32 = (int)nx, ny32 = (int)ny, tot32 = (int)tot;
+    for (int f = tid; f < tot32; f += nth) {
+      const int j = W == 1 ? 0 : (int)((unsigned)f / (unsigned)ny32);
+      const int i = f - j * ny32;
+      T* line = A + j * pitch;
+      const T* x = line + xo;
+      const int b = i + st.off;
+      T y = line[yo + i];
+      if (st.kind == K_UNIT) {
+        if (b >= 0 && b < nx32) y = st.sub ? y - x[b] : y + x[b];
+      } else if (b >= 0 && b + st.ntaps <= nx32) {
+        y = ip_interior(st, y, x, i);
+      } else {
+        y = ip_safe(st, y, x, b, nx);
+      }
+      line[yo + i] = y;
+    }
+    return;
+  }
   for (int64_t f = tid; f < tot; f += nth) {
     int j;
     int64_t i;
